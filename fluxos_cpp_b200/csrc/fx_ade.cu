@@ -1,0 +1,357 @@
+// FP64 advection-dispersion (ADE) step of FLUXOS-OVERLAND for sm_100a.
+//
+// ADEsolver_calc.cpp:27-291 re-scales every concentration to the new depth
+// (:47-73) and then sweeps the grid once in Gauss-Seidel order (:93-290):
+// cell (ix, iy) uses the already-updated concentration and limited fluxes of
+// (ix-1, iy) and (ix, iy-1). Only a wavefront reproduces that order exactly.
+//
+// Mapping. A warp owns a strip of 30 rows; lane t (< 30) owns row
+// ix0 + t and marches along iy with a skew of one column per lane, so at warp
+// step tau lane t updates (ix0 + t, tau - t + 1) and every lane's west
+// neighbour was updated by lane t-1 one step earlier:
+//   * the west carries (updated c, limited flux pfe, re-scaled c, dry flag)
+//     move lane t-1 -> t with one shuffle per step;
+//   * the south carries (updated c, limited flux qfn) stay in registers;
+//   * east / east-east / north / north-north inputs are prefetched by the
+//     owning lane two columns ahead and shuffled down; lanes 30 and 31 only
+//     prefetch the first two rows of the next strip.
+// The re-scale of :47-73 is pointwise, so it is applied to each record as it
+// is loaded; the bounds of :51-62 come from the pre-sweep value of the east
+// and north cells and the re-scaled value of the west and south cells.
+// Strips hand over through a small boundary buffer (per column: updated c,
+// pfe, re-scaled c of the strip's last row) and a release/acquire progress
+// counter; every wait is bounded and sets fx_ctl::error when it gives up.
+// All solutes of the step run in the same launch (independent chains).
+#include <cuda_runtime.h>
+
+#include "fx_common.cuh"
+
+namespace fxade {
+
+constexpr int ROWS = 30;      // rows per strip (lanes 0..29 compute)
+constexpr int WARPS = 4;      // warps per block
+constexpr int CHUNK = 8;      // steps between progress publications
+constexpr long long SPIN_LIMIT = 1LL << 20;  // polls (well under a second) before giving up
+
+struct Rec {
+  double c;   // concentration before the sweep (after dilution, before re-scale)
+  double b;   // re-scaled concentration (ADEsolver_calc.cpp:64-72)
+  double h;   // depth after the hydrodynamic update
+  double qx;  // fe_1 of the cell
+  double qy;  // fn_1 of the cell
+  int ld;     // ldry (1 = dry); ghost cells read 0
+};
+
+__device__ __forceinline__ Rec load_rec(const fx_dev& d, const double* A, int ix, int iy) {
+  Rec r;
+  r.c = 0.0;
+  r.b = 0.0;
+  r.h = 0.0;
+  r.qx = 0.0;
+  r.qy = 0.0;
+  r.ld = 0;
+  if (ix < 0 || ix > d.nr + 1 || iy < 0 || iy > d.nc + 1) return r;
+  const long long gi = fx_ix(d, ix, iy);
+  r.h = d.h[gi];
+  if (ix >= 1 && ix <= d.nr && iy >= 1 && iy <= d.nc) {
+    const uint8_t fl = d.flags[gi];
+    r.ld = fl & FX_F_LDRY;
+    const int ldp = (fl & FX_F_LDRY_PREV) ? 1 : 0;
+    const double c = A[gi];
+    r.c = c;
+    if (r.ld == 0 && ldp == 0) r.b = c * d.h0[gi] / r.h;
+    else if (r.ld == 1) r.b = 0.0;
+    else r.b = c;
+    r.qx = d.fe1[gi];
+    r.qy = d.fn1[gi];
+  }
+  return r;
+}
+
+__device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+__device__ __forceinline__ double shdn(double v, int k) { return __shfl_down_sync(0xffffffffu, v, k); }
+__device__ __forceinline__ double shup(double v, int k) { return __shfl_up_sync(0xffffffffu, v, k); }
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// One cell of the sweep, ADEsolver_calc.cpp:126-288, for a wet cell.
+__device__ __forceinline__ void ade_cell(const fx_dev& d, double D, double dt, bool last_row,
+                                         bool last_col, double hp, double he, double hn, double qxl,
+                                         double qyl, double fw, double fp, double fe, double fee,
+                                         double fs, double fn, double fnn, double pfw, double qfs,
+                                         int ldE, int ldW, int ldEE, int ldN, int ldS, int ldNN,
+                                         double cmax, double cmin, double& con, double& pfe_out,
+                                         double& qfn_out) {
+  const double nt = 1, sigc = 0.5;
+  const double dx = d.dxy, dy = d.dxy;
+  const double area = d.arbase, areae = d.arbase, arean = d.arbase;
+  const double ntp = nt;
+  double fem, pfde, hnue, hne;
+  if (ldE == 0) {  // :151-172
+    hnue = fmax(hp * nt * he * nt, .0001);
+    hne = sqrt(hnue) / sigc / dx * dy * D;
+    pfde = -hne * (fe - fp);
+    if (qxl > 0.0) {
+      if (ldW == 0) fem = -.125 * fw + .75 * fp + .375 * fe;
+      else fem = 0.5 * fp + 0.5 * fe;
+    } else {
+      if (ldEE == 0) fem = .375 * fp + .75 * fe - .125 * fee;
+      else fem = 0.5 * fp + 0.5 * fe;
+    }
+  } else {
+    fem = 0.;
+    pfde = 0.;
+  }
+  fem = fmax(0., fem);
+  if (last_row) fem = 0.0;  // :176-178, ghost concentration c(NROWS+1, iy) = 0
+  const double pfce = qxl * fem * dy;
+  double pfe = pfce + pfde;
+  if (pfe < 0) {  // :187-194
+    if (ldE == 0) {
+      const double cvolrate = -(fe * he) * areae / dt;
+      pfe = fmax(pfe, cvolrate);
+    } else {
+      pfe = 0.;
+    }
+  }
+  double fnm, qfdn, hnn;
+  if (ldN == 0) {  // :198-218
+    hnue = fmax(.0001, hp * ntp * hn * nt);
+    hnn = sqrt(hnue) / sigc / dy * dx * D;
+    qfdn = -hnn * (fn - fp);
+    if (qyl > 0.0) {
+      if (ldS == 0) fnm = -.125 * fs + .75 * fp + .375 * fn;
+      else fnm = 0.5 * fp + .5 * fn;
+    } else {
+      if (ldNN == 0) fnm = .375 * fp + .75 * fn - .125 * fnn;
+      else fnm = .5 * fp + .5 * fn;
+    }
+  } else {
+    fnm = 0.;
+    qfdn = 0.;
+  }
+  fnm = fmax(0., fnm);
+  if (last_col) fnm = 0.0;  // :223-225, ghost concentration c(ix, NCOLS+1) = 0
+  const double qfcn = qyl * fnm * dx;
+  double qfn = qfcn + qfdn;
+  if (qfn < 0) {  // :234-241
+    if (ldN == 0) {
+      const double cvolrate = -(fn * hn) * arean / dt;
+      qfn = fmax(qfn, cvolrate);
+    } else {
+      qfn = 0.;
+    }
+  }
+  const double cvolpot = (fp * hp) * area;  // :243-278
+  const double cvolrat = cvolpot / dt + pfw + qfs;
+  if (cvolrat > 0.0) {
+    if (pfe > 0. && qfn > 0.) {
+      if (pfe + qfn > cvolrat) {
+        const double cf = qfn / (pfe + qfn);
+        pfe = (1. - cf) * cvolrat;
+        qfn = cf * cvolrat;
+      }
+    } else if (pfe > 0.) {
+      pfe = fmin(pfe, (cvolrat - qfn));
+    } else if (qfn > 0.) {
+      qfn = fmin(qfn, (cvolrat - pfe));
+    }
+  } else {
+    if (pfe >= 0. && qfn < 0.) {
+      const double cbilan = cvolrat - qfn;
+      if (cbilan > 0.) pfe = fmin(pfe, cbilan);
+      else pfe = 0.;
+    } else if (pfe < 0. && qfn >= 0.) {
+      const double cbilan = cvolrat - pfe;
+      if (cbilan > 0.) qfn = fmin(qfn, cbilan);
+      else qfn = 0.;
+    } else if (pfe >= 0. && qfn >= 0.) {
+      pfe = 0.0;
+      qfn = 0.0;
+    }
+  }
+  const double dc = (pfw - pfe + qfs - qfn) * dt / area;  // :281-286
+  double cn = fp + dc / hp;
+  cn = fmin(cmax, cn);
+  cn = fmax(cmin, cn);
+  con = cn;
+  pfe_out = pfe;
+  qfn_out = qfn;
+}
+
+__global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips) {
+  const fx_ctl& cc = *d.ctl;
+  if (!cc.live || !cc.active || !d.ade || cc.it <= 1) return;  // :45,74-77
+  const double dt = cc.dtfl;
+  const unsigned epoch = (unsigned)cc.steps;
+  const int lane = threadIdx.x & 31;
+  const int wg = blockIdx.x * WARPS + (threadIdx.x >> 5);
+  const int nwarps = gridDim.x * WARPS;
+  const int units = nstrips * d.nchem;
+  const int T = d.nc + ROWS - 1;  // warp steps per strip
+  const long long bnd_stride = (long long)(d.nc + 2) * 3;
+
+  for (int u = wg; u < units; u += nwarps) {
+    const int k = u / nstrips, s = u % nstrips;
+    double* A = d.conc + k * d.plane;
+    const double D = d.dcoef[k];
+    const int ix0 = 1 + s * ROWS;
+    const int ix = ix0 + lane;
+    const bool compute_lane = lane < ROWS && ix <= d.nr;
+    unsigned long long* prog_prev = (s > 0) ? d.ade_prog + (long long)k * nstrips + (s - 1) : nullptr;
+    unsigned long long* prog_me = d.ade_prog + (long long)k * nstrips + s;
+    const double* bnd_in = d.ade_bnd + ((long long)k * nstrips + s) * bnd_stride;
+    double* bnd_out = (s + 1 < nstrips) ? d.ade_bnd + ((long long)k * nstrips + s + 1) * bnd_stride : nullptr;
+
+    // register pipeline: columns iy, iy+1, iy+2 of this lane's row
+    Rec cur = load_rec(d, A, ix, 1 - lane);
+    Rec n1 = load_rec(d, A, ix, 2 - lane);
+    Rec n2 = load_rec(d, A, ix, 3 - lane);
+    // carries: outputs of this lane's previous cell (its south cell for the
+    // next step, its west cell for lane + 1)
+    double o_c = 0.0, o_pfe = 0.0, o_b = 0.0, o_qfn = 0.0;
+    int o_ld = 0;
+    // boundary values of the chunk (lane j holds column tau0 + 1 + j)
+    double bw_c = 0.0, bw_pfe = 0.0, bw_b = 0.0;
+    int bw_ld = 0;
+    bool bail = false;
+
+    for (int tau = 0; tau < T; ++tau) {
+      if ((tau % CHUNK) == 0) {
+        if (prog_prev) {
+          int need = tau + CHUNK - 1 + ROWS;
+          if (need > T) need = T;
+          const unsigned long long want = ((unsigned long long)epoch << 32) | (unsigned)need;
+          long long it = 0;
+          for (;;) {
+            const unsigned long long v = ld_acquire(prog_prev);
+            if (__all_sync(0xffffffffu, v >= want)) break;
+            const bool stop = (++it > SPIN_LIMIT) || (*(volatile int*)&d.ctl->error != 0);
+            if (__any_sync(0xffffffffu, stop)) {
+              bail = true;
+              break;
+            }
+            __nanosleep(64);
+          }
+          if (__any_sync(0xffffffffu, bail)) {
+            if (lane == 0) atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
+            bail = true;
+            break;
+          }
+          const int iyb = tau + 1 + lane;
+          if (lane < CHUNK && iyb <= d.nc) {
+            const double* p = bnd_in + (long long)iyb * 3;
+            bw_c = __ldcg(p);
+            bw_pfe = __ldcg(p + 1);
+            bw_b = __ldcg(p + 2);
+            bw_ld = d.flags[fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
+          } else {
+            bw_c = bw_pfe = bw_b = 0.0;
+            bw_ld = 0;
+          }
+        }
+      }
+      const int iy = tau - lane + 1;
+      // east (lane+1's next column), east-east (lane+2's column after next)
+      const double E_c = shdn(n1.c, 1), E_b = shdn(n1.b, 1), E_h = shdn(n1.h, 1);
+      const int E_ld = __shfl_down_sync(0xffffffffu, n1.ld, 1);
+      double EE_b = shdn(n2.b, 2);
+      int EE_ld = __shfl_down_sync(0xffffffffu, n2.ld, 2);
+      // west: lane-1's outputs of the previous step, or the boundary
+      double W_c = shup(o_c, 1), W_pfe = shup(o_pfe, 1), W_b = shup(o_b, 1);
+      int W_ld = __shfl_up_sync(0xffffffffu, o_ld, 1);
+      {
+        const int j = tau % CHUNK;
+        const double t_c = shfl_d(bw_c, j), t_pfe = shfl_d(bw_pfe, j), t_b = shfl_d(bw_b, j);
+        const int t_ld = __shfl_sync(0xffffffffu, bw_ld, j);
+        if (lane == 0) {
+          // Strip 0's west neighbour is the ghost row 0: c = 0, pfe = the
+          // ghost convective flux c(0,iy)*fe_1(0,iy)*dy = 0 (:106-116).
+          W_c = t_c;
+          W_pfe = t_pfe;
+          W_b = t_b;
+          W_ld = t_ld;
+        }
+      }
+      if (compute_lane && iy >= 1 && iy <= d.nc) {
+        const long long gi = fx_ix(d, ix, iy);
+        const bool last_row = ix == d.nr, last_col = iy == d.nc;
+        double out_c, pfe = 0.0, qfn = 0.0;
+        if (last_row) {  // iee = min(ix+2, NROWS+1) = ie
+          EE_b = E_b;
+          EE_ld = E_ld;
+        }
+        const double NN_b = last_col ? n1.b : n2.b;  // inn = min(iy+2, NCOLS+1)
+        const int NN_ld = last_col ? n1.ld : n2.ld;
+        if (last_row && last_col) {
+          out_c = cur.b;  // the sweep stops one cell short (:93)
+        } else if (cur.ld == 1) {
+          out_c = 0.0;  // :119-124
+        } else {
+          const double cmax = fmax(W_b, fmax(E_c, fmax(o_b, n1.c)));
+          const double cmin = fmin(W_b, fmin(E_c, fmin(o_b, n1.c)));
+          ade_cell(d, D, dt, last_row, last_col, cur.h, E_h, n1.h, cur.qx, cur.qy, W_c, cur.b, E_b,
+                   EE_b, o_c, n1.b, NN_b, W_pfe, o_qfn, E_ld, W_ld, EE_ld, n1.ld, o_ld, NN_ld, cmax,
+                   cmin, out_c, pfe, qfn);
+        }
+        A[gi] = out_c;
+        if (lane == ROWS - 1 && bnd_out) {
+          double* p = bnd_out + (long long)iy * 3;
+          p[0] = out_c;
+          p[1] = pfe;
+          p[2] = cur.b;
+        }
+        o_c = out_c;
+        o_pfe = pfe;
+        o_b = cur.b;
+        o_ld = cur.ld;
+        o_qfn = qfn;
+      } else if (iy < 1) {
+        // not started: the south neighbour of column 1 is the ghost column
+        o_c = 0.0;
+        o_pfe = 0.0;
+        o_b = 0.0;
+        o_ld = 0;
+        o_qfn = 0.0;
+      }
+      // publish progress (lane 29 owns the boundary values)
+      if (((tau + 1) % CHUNK) == 0 || tau + 1 == T) {
+        if (lane == ROWS - 1) {
+          __threadfence();
+          st_release(prog_me, ((unsigned long long)epoch << 32) | (unsigned)(tau + 1));
+        }
+      }
+      cur = n1;
+      n1 = n2;
+      n2 = load_rec(d, A, ix, tau - lane + 4);
+    }
+    if (bail) return;
+  }
+}
+
+}  // namespace fxade
+
+int fx_ade_rows_per_strip() { return fxade::ROWS; }
+int fx_ade_threads_per_block() { return fxade::WARPS * 32; }
+
+void fx_launch_ade(const fx_dev& d, int nstrips, int nblocks, cudaStream_t s) {
+  fxade::k_ade_sweep<<<nblocks, fxade::WARPS * 32, 0, s>>>(d, nstrips);
+}
+
+int fx_ade_max_blocks(int* out) {
+  int dev = 0, nsm = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fxade::k_ade_sweep, fxade::WARPS * 32, 0) !=
+      cudaSuccess)
+    return -1;
+  *out = per * nsm;
+  return 0;
+}

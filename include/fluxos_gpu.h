@@ -1,0 +1,160 @@
+/* fluxos_gpu.h: C ABI of libfluxos_gpu.so, the B200 (sm_100a) implementation
+ * of the FLUXOS-OVERLAND explicit time step.
+ *
+ * Plain C types only: sizes are ints, grids are host pointers to the
+ * reference's GlobVar layout, i.e. (NROWS+2) x (NCOLS+2) values, column-major
+ * with irow fastest, ghost ring included (src/fluxos/GlobVar.h:31-74). Every
+ * call returns FX_OK (0) or a negative FX_ERR_* code and never throws; the
+ * message of the last failure is fx_last_error(). A context owns its device
+ * memory and one CUDA stream; use one host thread per context. Contexts are
+ * independent of each other.
+ *
+ * Reference interfaces replaced (DiogoCostaPT/FLUXOS_cpp, src/fluxos/):
+ *   fx_step / fx_run_to_print : one or more iterations of the step loop
+ *       main.cpp:271-470, i.e. the Courant scan main.cpp:300-325,
+ *       add_meteo (common.cpp:164, common.h:50-67),
+ *       hydrodynamics_calc (hydrodynamics_calc.h:24) and
+ *       adesolver_calc (ADEsolver_calc.h:25)
+ *   fx_open_modset : the start-up main.cpp:87-262 with read_modset,
+ *       read_geo, read_meteo (read_functions.h:25-43) and initiation
+ *       (initiate.h)
+ *   fx_write_results : write_results (write_results.cpp:30)
+ *   fx_run : the whole program `fluxos <modset.json>` (main.cpp:70)
+ */
+#ifndef FLUXOS_GPU_H
+#define FLUXOS_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FX_OK 0
+#define FX_ERR_ARG -1    /* bad argument or size */
+#define FX_ERR_CUDA -2   /* a CUDA runtime call failed (message has the call) */
+#define FX_ERR_IO -3     /* an input file could not be read or an output written */
+#define FX_ERR_STATE -4  /* call out of order (e.g. stepping a finished run) */
+#define FX_ERR_DEVICE -5 /* a kernel raised its error flag (a bounded wait gave up) */
+#define FX_ERR_NOMEM -6  /* device allocation failed */
+
+#define FX_MAX_CHEM 8
+
+typedef struct fx_ctx fx_ctx;
+
+/* Domain (GlobVar.h:75-76,104; read_functions.cpp:130-139). */
+typedef struct fx_grid {
+  int nrows;     /* NROWS: interior cells along irow */
+  int ncols;     /* NCOLS: interior cells along icol */
+  int dxy;       /* cell size [m], an integer as in the reference */
+  int nchem;     /* solutes, 1..FX_MAX_CHEM (the reference has 1) */
+  double nodata; /* NODATA_VALUE */
+  double xll;    /* XLLCORNER */
+  double yll;    /* YLLCORNER */
+} fx_grid;
+
+/* Physics and run control. */
+typedef struct fx_params {
+  double hdry;       /* dry threshold; the reference sets it to ks(1,1) (main.cpp:259) */
+  double ks;         /* ROUGNESS_HEIGHT of interior cells */
+  double ntim;       /* run while tim <= ntim (main.cpp:192,271) */
+  double print_step; /* PRINT_STEP [s] */
+  double print_next; /* first output time (main.cpp:260-261) */
+  double tim;        /* starting clock (0 in the reference) */
+  double h_min_print;/* H_MIN_TO_PRINT as the reference stores it (an integer) */
+  int ade;           /* EXTERNAL_MODULES.ADE_TRANSPORT.STATUS */
+  int volrat_mode;   /* domain-edge weir: 0 = weir formula (default), 1 = closed */
+  double d_coef[FX_MAX_CHEM]; /* dispersion coefficient per solute */
+} fx_params;
+
+/* Clock and status read back from the device. */
+typedef struct fx_status {
+  double tim;           /* simulated clock [s] */
+  double dtfl;          /* last dt [s] */
+  double print_next;    /* next output time [s] */
+  double hpall;         /* max wet depth of the last Courant scan */
+  long long steps;      /* steps executed since creation */
+  int it;               /* solver iterations (main.cpp:387) */
+  int print_pending;    /* tim >= print_next: write results, then fx_print_done */
+  int finished;         /* tim > ntim: the run is over */
+  int device_error;     /* nonzero when a kernel gave up a bounded wait */
+  int forcing_overrun;  /* the forcing table had no row later than tim */
+} fx_status;
+
+/* --- context ------------------------------------------------------------ */
+int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out);
+void fx_destroy(fx_ctx* ctx);
+const char* fx_last_error(const fx_ctx* ctx); /* ctx may be NULL: last global error */
+int fx_device_bytes(const fx_ctx* ctx, long long* bytes); /* device memory held */
+
+/* --- state ---------------------------------------------------------------
+ * Field names: "z" "zb" "h" "qx" "qy" "twet" "h0" "fe_1" "fe_2" "fe_3"
+ * "fn_1" "fn_2" "fn_3" "conc" (solute 0) "conc1".."conc7".
+ * Uploads take the full (nrows+2) x (ncols+2) grid; fx_upload_flags takes the
+ * float flag grids ldry and innerNeumannBCWeir (wall) of GlobVar. After the
+ * state is complete call fx_prepare once (it runs the first Courant scan). */
+int fx_upload(fx_ctx* ctx, const char* field, const double* host_grid);
+int fx_download(fx_ctx* ctx, const char* field, double* host_grid);
+int fx_upload_flags(fx_ctx* ctx, const float* ldry, const float* wall);
+int fx_download_flags(fx_ctx* ctx, float* ldry, float* ldry_prev, float* wall);
+/* Forcing table of GlobVar::meteo: 2000 rows x 3 columns (time [s], rate
+ * [mm/day], concentration), column-major float as arma::fmat(2000,3).
+ * has_meteo = 0 means no METEO_FILE (add_meteo returns at common.cpp:190). */
+int fx_set_forcing(fx_ctx* ctx, const float* table_2000x3, int has_meteo);
+/* Extensions without a reference counterpart (NULL switches them off):
+ * per-cell Manning n (semi-implicit friction after the update) and a
+ * per-cell multiplier of the melt rate. Full grids as for fx_upload. */
+int fx_set_manning(fx_ctx* ctx, const double* n_grid);
+int fx_set_melt_field(fx_ctx* ctx, const double* mult_grid);
+/* Options: "store_all_fluxes" (1 keeps fe_2/fe_3/fn_2/fn_3 current on the
+ * device every step; 0, the default, skips those stores for cells that end a
+ * step wet, whose values are never read back by a later step). */
+int fx_set_option(fx_ctx* ctx, const char* name, long long value);
+int fx_prepare(fx_ctx* ctx);
+
+/* --- stepping ------------------------------------------------------------ */
+/* Run up to nsteps steps; stops early when an output is due or the run ends. */
+int fx_step(fx_ctx* ctx, int nsteps, fx_status* st);
+/* Run until an output is due or the run ends. */
+int fx_run_to_print(fx_ctx* ctx, fx_status* st);
+/* Acknowledge a due output: print_next += print_step (main.cpp:458). */
+int fx_print_done(fx_ctx* ctx);
+int fx_get_status(fx_ctx* ctx, fx_status* st);
+/* The context's CUDA stream (a cudaStream_t), for callers that time it. */
+void* fx_stream(fx_ctx* ctx);
+/* Device time of n steps in milliseconds, measured with CUDA events on the
+ * context's stream, plus the summed time of the hydro and ADE kernels
+ * measured launch by launch (for roofline accounting). */
+int fx_time_steps(fx_ctx* ctx, int nsteps, double* ms_total, double* ms_hydro, double* ms_ade);
+
+/* --- the reference's file surface (host C++) ---------------------------- */
+/* read_geo's wall/roughness step (read_functions.cpp:175-225) and the zero
+ * initial state of initiation (initiate.cpp:43-107,159-228) from the DEM
+ * values as read (float-rounded, GlobVar layout, ghost ring 0); uploads the
+ * state and runs fx_prepare. */
+int fx_initiate(fx_ctx* ctx, const double* zb_raw);
+/* Host-only part of the start-up below (no GPU needed): parse the modset,
+ * DEM and forcing files and build the initial state exactly as main.cpp:
+ * 104-262 does. Call once with all array pointers NULL to fill g and p (the
+ * sizes), then with arrays of (nrows+2)*(ncols+2) elements and a 3*2000
+ * forcing table. */
+int fx_load_modset(const char* modset_path, fx_grid* g, fx_params* p, double* zb, double* z,
+                   double* h, double* qx, double* qy, double* twet, double* conc, float* ldry,
+                   float* wall, float* table_2000x3, int* has_meteo);
+/* Start-up of main.cpp:87-262 from a modset file: reads the master file
+ * (with comments), the ESRI ASCII DEM, the forcing CSV, applies initiation
+ * (bed averaging, zero or restart initial state, ghost ring), uploads. */
+int fx_open_modset(const char* modset_path, fx_ctx** out);
+/* write_results (write_results.cpp:30-101): Results/<t>.txt of the current
+ * state; path NULL means <OUTPUT_FOLDER>/<print_next>.txt. */
+int fx_write_results(fx_ctx* ctx, const char* path);
+/* The writer itself on host grids (no GPU needed). */
+int fx_write_results_host(const char* path, int nrows, int ncols, int dxy, double xll, double yll,
+                          double h_min_print, const double* z, const double* zb, const double* h,
+                          const double* qx, const double* qy, const double* conc, const double* fe_1,
+                          const double* fn_1, const double* twet);
+/* The whole program: open, step, write every output, close. */
+int fx_run(const char* modset_path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

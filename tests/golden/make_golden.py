@@ -1,0 +1,140 @@
+"""Regenerate the golden fixtures in this folder from the FLUXOS reference.
+
+Run from the repository root where the reference tree is mounted:
+
+    make -C oracle all && python tests/golden/make_golden.py
+
+Each case is a small seeded scenario. Its input files are written exactly as
+the reference reads them, and the reference sources compiled in
+oracle/_ref/ are stepped through the harness (oracle/ref_harness.cpp). State
+snapshots are saved at the listed step counts. One case also keeps the
+Results/<t>.txt files that the whole reference program (oracle/_ref/fluxos_ref)
+writes. The fixtures hold the input text, so tests need neither the reference
+nor this script.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from fluxos_cpp_b200 import scenarios as S  # noqa: E402
+import pyoracle as P  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SNAP_GRIDS = ("z", "h", "qx", "qy", "conc", "fe_1", "fe_2", "fe_3", "fn_1", "fn_2", "fn_3",
+              "twet", "h0", "ldry", "ldry_prev", "zb", "wall", "ks")
+
+
+def case_plane_walls() -> dict:
+    sc = S.plane_scenario(24, 20, seed=0)
+    sc.horizon = 6000.0
+    sc.meteo = ((0.0, 40.0, 1.0), (6000.0, 40.0, 1.0))
+    sc.dem[3:6, 4] = -9999.0
+    sc.dem[10, 2:9] = 0.0
+    return dict(sc=sc, wet=None, steps=(1, 100, 1000, 5000), mode=0, results=True)
+
+
+def _patch(nr, nc, seed):
+    rng = np.random.default_rng(seed)
+    h = np.where(rng.random((nr, nc)) < 0.6, rng.uniform(0, 0.05, (nr, nc)), 0.0)
+    qx = rng.normal(0, 0.002, (nr, nc)) * (h > 0)
+    qy = rng.normal(0, 0.002, (nr, nc)) * (h > 0)
+    c = rng.uniform(0, 2, (nr, nc)) * (h > 0)
+    return dict(h=h, qx=qx, qy=qy, conc=[c])
+
+
+def case_patchwork(mode: int) -> dict:
+    sc = S.plane_scenario(24, 20, seed=1)
+    sc.horizon = 3000.0
+    sc.dem[6, 3:7] = -9999.0
+    return dict(sc=sc, wet=_patch(24, 20, 3), steps=(1, 10, 100, 300), mode=mode, results=False)
+
+
+def case_dambreak() -> dict:
+    nr, nc = 32, 28
+    dem = np.full((nr, nc), 100.0, dtype=np.float32)
+    sc = S.Scenario(name="dambreak", dem=dem, dxy=1, meteo=((0.0, 0.0, 0.0), (600.0, 0.0, 0.0)),
+                    horizon=600.0, print_step=60, ks=0.001, ade=True, d_coef=0.1)
+    yy, xx = np.mgrid[0:nr, 0:nc]
+    r = np.hypot(yy - nr / 2 + 0.5, xx - nc / 2 + 0.5)
+    h = np.where(r < 8.0, 0.5, 0.0)
+    return dict(sc=sc, wet=dict(h=h, qx=np.zeros_like(h), qy=np.zeros_like(h),
+                                conc=[np.where(r < 8.0, 1.0, 0.0)]),
+                steps=(1, 20, 200), mode=0, results=False)
+
+
+CASES = {
+    "plane_walls": case_plane_walls,
+    "patchwork_weir": lambda: case_patchwork(0),
+    "patchwork_closed": lambda: case_patchwork(1),
+    "dambreak": case_dambreak,
+}
+
+
+def build_case(name: str, spec: dict) -> None:
+    sc, mode = spec["sc"], spec["mode"]
+    work = tempfile.mkdtemp(prefix=f"golden_{name}_")
+    modset = sc.write(work)
+    out = {}
+    with open(os.path.join(work, "dem.asc")) as f:
+        out["dem_asc"] = np.array(f.read())
+    with open(os.path.join(work, "meteo.csv")) as f:
+        out["meteo_csv"] = np.array(f.read())
+    meta = dict(name=name, nrows=sc.nrows, ncols=sc.ncols, dxy=sc.dxy, nodata=sc.nodata,
+                print_step=sc.print_step, ks=sc.ks, ade=sc.ade, d_coef=sc.d_coef,
+                h_min_print=sc.h_min_print, volrat_mode=mode, steps=list(spec["steps"]),
+                wet=spec["wet"] is not None)
+    ref = P.RefRun(modset, sc, mode)
+    if spec["wet"] is not None:
+        w = spec["wet"]
+        ref.apply_wet_start(w["h"], w["qx"], w["qy"], w["conc"])
+        for k in ("h", "qx", "qy"):
+            out[f"wet_{k}"] = w[k]
+        out["wet_conc0"] = w["conc"][0]
+    done = 0
+    scal = {}
+    for target in spec["steps"]:
+        while done < target:
+            ref.step()
+            if ref.print_due():
+                ref.print_done()
+            done += 1
+        for g in SNAP_GRIDS:
+            out[f"s{target}_{g}"] = ref.grid(g).copy()
+        scal[str(target)] = {k: ref.scalar(k) for k in ("tim", "dtfl", "it", "hpall", "print_next")}
+    meta["scalars"] = scal
+    if spec["results"]:
+        work2 = tempfile.mkdtemp(prefix=f"golden_{name}_main_")
+        modset2 = sc.write(work2)
+        r = subprocess.run([P.REF_BIN, modset2], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr)
+        res = os.path.join(work2, "Results")
+        files = sorted(os.listdir(res), key=lambda s: int(s.split(".")[0]))
+        meta["results"] = files
+        for fn in files:
+            with open(os.path.join(res, fn)) as f:
+                out[f"results_{fn}"] = np.array(f.read())
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, "snapshots", spec["steps"], "results" if spec["results"] else "")
+
+
+def main() -> None:
+    if not P.ref_available(0):
+        sys.exit("oracle/_ref is not built: run `make -C oracle all` with the reference present")
+    for name, fn in CASES.items():
+        build_case(name, fn())
+
+
+if __name__ == "__main__":
+    main()
