@@ -31,7 +31,21 @@ namespace fxade {
 constexpr int ROWS = 30;      // rows per strip (lanes 0..29 compute)
 constexpr int WARPS = 4;      // warps per block
 constexpr int CHUNK = 8;      // steps between progress publications
+constexpr int RING = 16;      // per-lane prefetch slots (a power of two)
+constexpr int DIST = 12;      // prefetch distance in columns (< RING)
 constexpr long long SPIN_LIMIT = 1LL << 20;  // polls (well under a second) before giving up
+
+// Per-lane ring of prefetched cells, filled by cp.async (asynchronous
+// global -> shared copies: the loads of a future column are in flight while
+// the lane computes, and no register waits on them).
+struct Ring {
+  double c[RING][32];    // concentration before the sweep
+  double h0[RING][32];   // depth after forcing, before the update (re-scale)
+  double h[RING][32];    // depth after the update
+  double fe1[RING][32];  // fe_1
+  double fn1[RING][32];  // fn_1
+  unsigned fl[RING][32]; // the 4-byte word holding the cell's flag byte
+};
 
 struct Rec {
   double c;   // concentration before the sweep (after dilution, before re-scale)
@@ -42,7 +56,39 @@ struct Rec {
   int ld;     // ldry (1 = dry); ghost cells read 0
 };
 
-__device__ __forceinline__ Rec load_rec(const fx_dev& d, const double* A, int ix, int iy) {
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 8 : 0;  // 0 source bytes: the slot is zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Issue the copies of cell (ix, iy) into ring slot `slot` of this lane.
+__device__ __forceinline__ void prefetch(const fx_dev& d, const double* A, Ring& R, int lane, int ix,
+                                         int iy) {
+  const int slot = iy & (RING - 1);
+  const bool inr = ix >= 0 && ix <= d.nr + 1 && iy >= 0 && iy <= d.nc + 1;
+  const long long gi = inr ? fx_ix(d, ix, iy) : 0;
+  cp_async8(&R.c[slot][lane], A + gi, inr);
+  cp_async8(&R.h0[slot][lane], d.h0 + gi, inr);
+  cp_async8(&R.h[slot][lane], d.h + gi, inr);
+  cp_async8(&R.fe1[slot][lane], d.fe1 + gi, inr);
+  cp_async8(&R.fn1[slot][lane], d.fn1 + gi, inr);
+  cp_async4(&R.fl[slot][lane], d.flags + (gi & ~3LL), inr);
+}
+
+// The record of cell (ix, iy) from its ring slot, re-scaled as
+// ADEsolver_calc.cpp:64-72 does; ghost cells carry only their depth.
+__device__ __forceinline__ Rec make_rec(const fx_dev& d, const Ring& R, int lane, int ix, int iy) {
   Rec r;
   r.c = 0.0;
   r.b = 0.0;
@@ -51,19 +97,20 @@ __device__ __forceinline__ Rec load_rec(const fx_dev& d, const double* A, int ix
   r.qy = 0.0;
   r.ld = 0;
   if (ix < 0 || ix > d.nr + 1 || iy < 0 || iy > d.nc + 1) return r;
-  const long long gi = fx_ix(d, ix, iy);
-  r.h = d.h[gi];
+  const int slot = iy & (RING - 1);
+  r.h = R.h[slot][lane];
   if (ix >= 1 && ix <= d.nr && iy >= 1 && iy <= d.nc) {
-    const uint8_t fl = d.flags[gi];
+    const long long gi = fx_ix(d, ix, iy);
+    const unsigned fl = (R.fl[slot][lane] >> (8 * (unsigned)(gi & 3))) & 0xffu;
     r.ld = fl & FX_F_LDRY;
     const int ldp = (fl & FX_F_LDRY_PREV) ? 1 : 0;
-    const double c = A[gi];
+    const double c = R.c[slot][lane];
     r.c = c;
-    if (r.ld == 0 && ldp == 0) r.b = c * d.h0[gi] / r.h;
+    if (r.ld == 0 && ldp == 0) r.b = c * R.h0[slot][lane] / r.h;
     else if (r.ld == 1) r.b = 0.0;
     else r.b = c;
-    r.qx = d.fe1[gi];
-    r.qy = d.fn1[gi];
+    r.qx = R.fe1[slot][lane];
+    r.qy = R.fn1[slot][lane];
   }
   return r;
 }
@@ -186,13 +233,34 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, double D, double dt, b
   qfn_out = qfn;
 }
 
+// Wait until strip progress reaches `need` warp steps of this epoch; false
+// if the wait gave up (the error flag is then set).
+__device__ __forceinline__ bool wait_progress(const fx_dev& d, const unsigned long long* prog, unsigned epoch,
+                                              int need) {
+  const unsigned long long want = ((unsigned long long)epoch << 32) | (unsigned)need;
+  long long it = 0;
+  for (;;) {
+    const unsigned long long v = ld_acquire(prog);
+    if (__all_sync(0xffffffffu, v >= want)) return true;
+    const bool stop = (++it > SPIN_LIMIT) || (*(volatile int*)&d.ctl->error != 0);
+    if (__any_sync(0xffffffffu, stop)) {
+      if ((threadIdx.x & 31) == 0) atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
+      return false;
+    }
+    __nanosleep(64);
+  }
+}
+
 __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const fx_ctl& cc = *d.ctl;
   if (!cc.live || !cc.active || !d.ade || cc.it <= 1) return;  // :45,74-77
   const double dt = cc.dtfl;
   const unsigned epoch = (unsigned)cc.steps;
   const int lane = threadIdx.x & 31;
-  const int wg = blockIdx.x * WARPS + (threadIdx.x >> 5);
+  const int wib = threadIdx.x >> 5;
+  Ring& R = reinterpret_cast<Ring*>(smem_raw)[wib];
+  const int wg = blockIdx.x * WARPS + wib;
   const int nwarps = gridDim.x * WARPS;
   const int units = nstrips * d.nchem;
   const int T = d.nc + ROWS - 1;  // warp steps per strip
@@ -205,60 +273,78 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
     const int ix0 = 1 + s * ROWS;
     const int ix = ix0 + lane;
     const bool compute_lane = lane < ROWS && ix <= d.nr;
-    unsigned long long* prog_prev = (s > 0) ? d.ade_prog + (long long)k * nstrips + (s - 1) : nullptr;
+    const unsigned long long* prog_prev =
+        (s > 0) ? d.ade_prog + (long long)k * nstrips + (s - 1) : nullptr;
     unsigned long long* prog_me = d.ade_prog + (long long)k * nstrips + s;
     const double* bnd_in = d.ade_bnd + ((long long)k * nstrips + s) * bnd_stride;
-    double* bnd_out = (s + 1 < nstrips) ? d.ade_bnd + ((long long)k * nstrips + s + 1) * bnd_stride : nullptr;
+    double* bnd_out =
+        (s + 1 < nstrips) ? d.ade_bnd + ((long long)k * nstrips + s + 1) * bnd_stride : nullptr;
 
-    // register pipeline: columns iy, iy+1, iy+2 of this lane's row
-    Rec cur = load_rec(d, A, ix, 1 - lane);
-    Rec n1 = load_rec(d, A, ix, 2 - lane);
-    Rec n2 = load_rec(d, A, ix, 3 - lane);
+    // prime the ring: columns iy0 .. iy0 + DIST + 2 of this lane's row
+    const int iy0 = 1 - lane;
+    __syncwarp();
+    for (int j = 0; j < DIST + 3; ++j) {
+      prefetch(d, A, R, lane, ix, iy0 + j);
+      cp_commit();
+    }
+    cp_wait<0>();
+    Rec cur = make_rec(d, R, lane, ix, iy0);
+    Rec n1 = make_rec(d, R, lane, ix, iy0 + 1);
+    Rec n2 = make_rec(d, R, lane, ix, iy0 + 2);
     // carries: outputs of this lane's previous cell (its south cell for the
     // next step, its west cell for lane + 1)
     double o_c = 0.0, o_pfe = 0.0, o_b = 0.0, o_qfn = 0.0;
     int o_ld = 0;
-    // boundary values of the chunk (lane j holds column tau0 + 1 + j)
-    double bw_c = 0.0, bw_pfe = 0.0, bw_b = 0.0;
-    int bw_ld = 0;
+    // west-boundary values of the current and the next chunk (lane j holds
+    // column chunk_start + 1 + j); strip 0's west neighbour is the ghost row 0:
+    // c = 0, pfe = the ghost convective flux c(0,iy)*fe_1(0,iy)*dy = 0 (:106-116)
+    double bw_c = 0.0, bw_pfe = 0.0, bw_b = 0.0, bn_c = 0.0, bn_pfe = 0.0, bn_b = 0.0;
+    int bw_ld = 0, bn_ld = 0;
     bool bail = false;
+    if (prog_prev) {
+      if (!wait_progress(d, prog_prev, epoch, min(CHUNK - 1 + ROWS, T))) {
+        bail = true;
+      } else {
+        const int iyb = 1 + lane;
+        if (lane < CHUNK && iyb <= d.nc) {
+          const double* p = bnd_in + (long long)iyb * 3;
+          bn_c = __ldcg(p);
+          bn_pfe = __ldcg(p + 1);
+          bn_b = __ldcg(p + 2);
+          bn_ld = d.flags[fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
+        }
+      }
+    }
 
-    for (int tau = 0; tau < T; ++tau) {
+    for (int tau = 0; tau < T && !bail; ++tau) {
       if ((tau % CHUNK) == 0) {
-        if (prog_prev) {
-          int need = tau + CHUNK - 1 + ROWS;
-          if (need > T) need = T;
-          const unsigned long long want = ((unsigned long long)epoch << 32) | (unsigned)need;
-          long long it = 0;
-          for (;;) {
-            const unsigned long long v = ld_acquire(prog_prev);
-            if (__all_sync(0xffffffffu, v >= want)) break;
-            const bool stop = (++it > SPIN_LIMIT) || (*(volatile int*)&d.ctl->error != 0);
-            if (__any_sync(0xffffffffu, stop)) {
-              bail = true;
-              break;
-            }
-            __nanosleep(64);
-          }
-          if (__any_sync(0xffffffffu, bail)) {
-            if (lane == 0) atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
+        bw_c = bn_c;
+        bw_pfe = bn_pfe;
+        bw_b = bn_b;
+        bw_ld = bn_ld;
+        if (prog_prev && tau + CHUNK < T) {
+          // the next chunk's boundary: wait for it now, use it in CHUNK steps
+          if (!wait_progress(d, prog_prev, epoch, min(tau + 2 * CHUNK - 1 + ROWS, T))) {
             bail = true;
             break;
           }
-          const int iyb = tau + 1 + lane;
+          const int iyb = tau + CHUNK + 1 + lane;
+          bn_c = bn_pfe = bn_b = 0.0;
+          bn_ld = 0;
           if (lane < CHUNK && iyb <= d.nc) {
             const double* p = bnd_in + (long long)iyb * 3;
-            bw_c = __ldcg(p);
-            bw_pfe = __ldcg(p + 1);
-            bw_b = __ldcg(p + 2);
-            bw_ld = d.flags[fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
-          } else {
-            bw_c = bw_pfe = bw_b = 0.0;
-            bw_ld = 0;
+            bn_c = __ldcg(p);
+            bn_pfe = __ldcg(p + 1);
+            bn_b = __ldcg(p + 2);
+            bn_ld = d.flags[fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
           }
         }
       }
       const int iy = tau - lane + 1;
+      // keep DIST columns in flight: column iy + DIST + 3 now, column iy + 3
+      // must have landed by the end of this step
+      prefetch(d, A, R, lane, ix, iy + DIST + 3);
+      cp_commit();
       // east (lane+1's next column), east-east (lane+2's column after next)
       const double E_c = shdn(n1.c, 1), E_b = shdn(n1.b, 1), E_h = shdn(n1.h, 1);
       const int E_ld = __shfl_down_sync(0xffffffffu, n1.ld, 1);
@@ -272,8 +358,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
         const double t_c = shfl_d(bw_c, j), t_pfe = shfl_d(bw_pfe, j), t_b = shfl_d(bw_b, j);
         const int t_ld = __shfl_sync(0xffffffffu, bw_ld, j);
         if (lane == 0) {
-          // Strip 0's west neighbour is the ghost row 0: c = 0, pfe = the
-          // ghost convective flux c(0,iy)*fe_1(0,iy)*dy = 0 (:106-116).
           W_c = t_c;
           W_pfe = t_pfe;
           W_b = t_b;
@@ -328,10 +412,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
           st_release(prog_me, ((unsigned long long)epoch << 32) | (unsigned)(tau + 1));
         }
       }
+      cp_wait<DIST>();
       cur = n1;
       n1 = n2;
-      n2 = load_rec(d, A, ix, tau - lane + 4);
+      n2 = make_rec(d, R, lane, ix, iy + 3);
     }
+    cp_wait<0>();
     if (bail) return;
   }
 }
@@ -340,16 +426,20 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
 
 int fx_ade_rows_per_strip() { return fxade::ROWS; }
 int fx_ade_threads_per_block() { return fxade::WARPS * 32; }
+static const size_t kAdeSmem = sizeof(fxade::Ring) * fxade::WARPS;
 
 void fx_launch_ade(const fx_dev& d, int nstrips, int nblocks, cudaStream_t s) {
-  fxade::k_ade_sweep<<<nblocks, fxade::WARPS * 32, 0, s>>>(d, nstrips);
+  fxade::k_ade_sweep<<<nblocks, fxade::WARPS * 32, kAdeSmem, s>>>(d, nstrips);
 }
 
 int fx_ade_max_blocks(int* out) {
   int dev = 0, nsm = 0, per = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fxade::k_ade_sweep, fxade::WARPS * 32, 0) !=
+  if (cudaFuncSetAttribute(fxade::k_ade_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdeSmem) !=
+      cudaSuccess)
+    return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fxade::k_ade_sweep, fxade::WARPS * 32, kAdeSmem) !=
       cudaSuccess)
     return -1;
   *out = per * nsm;

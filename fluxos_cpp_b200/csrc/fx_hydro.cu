@@ -61,6 +61,23 @@ __device__ __forceinline__ double fx_pow15(double h) {
   return p + (pe + h * slo);
 }
 
+// Cube root of x >= 0 by Newton iteration on the mantissa, using only
+// frexp/ldexp and IEEE +,-,*,/, so the oracle's C (ox_cbrt) computes the
+// same bits. Used by the Manning extension only.
+__device__ __forceinline__ double fx_cbrt(double x) {
+  if (!(x > 0.0) || isinf(x)) return x;
+  int e;
+  double m = frexp(x, &e);
+  int r = e % 3;
+  if (r < 0) r += 3;
+  m = ldexp(m, r);
+  e -= r;
+  double y = 0.5 + 0.35 * m;
+#pragma unroll 1
+  for (int i = 0; i < 7; ++i) y = y - (y * y * y - m) / (3.0 * y * y);
+  return ldexp(y, e / 3);
+}
+
 __device__ __forceinline__ int sidx(int sr, int sc) { return sc * SX + sr; }
 
 // solver_wetdomain.cpp:27-342 for the flux cell at stencil (sr, sc).
@@ -599,7 +616,7 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
       const double n = d.manning[gi];
       if (n != 0.0) {
         const double qm = sqrt(qx * qx + qy * qy);
-        const double h73 = h * h * cbrt(h);
+        const double h73 = h * h * fx_cbrt(h);
         const double den = 1.0 + dtl * d.gaccl * n * n * qm / h73;
         qx = qx / den;
         qy = qy / den;

@@ -890,6 +890,22 @@ void ox_hydrodynamics(ox_state* s) {
   }
 }
 
+/* Cube root of x >= 0 by Newton iteration on the mantissa, using only
+ * frexp/ldexp and IEEE +,-,*,/ (no libm approximation), so the CUDA path
+ * (fx_hydro.cu, fx_cbrt) computes the same bits. */
+static double ox_cbrt(double x) {
+  if (!(x > 0.0) || isinf(x)) return x;
+  int e;
+  double m = frexp(x, &e);
+  int r = e % 3;
+  if (r < 0) r += 3;
+  m = ldexp(m, r);
+  e -= r;
+  double y = 0.5 + 0.35 * m;
+  for (int i = 0; i < 7; ++i) y = y - (y * y * y - m) / (3.0 * y * y);
+  return ldexp(y, e / 3);
+}
+
 /* Extension (no reference counterpart): semi-implicit Manning friction on
  * wet, non-wall cells after the hydrodynamic update,
  *   q <- q / (1 + dt g n^2 |q| / h^(7/3)).
@@ -904,7 +920,7 @@ void ox_manning(ox_state* s) {
       if (s->ldry[i] != 0.0f || s->wall[i] != 0.0f || n == 0.0) continue;
       double hp = s->h[i];
       double qm = sqrt(s->qx[i] * s->qx[i] + s->qy[i] * s->qy[i]);
-      double h73 = hp * hp * cbrt(hp);
+      double h73 = hp * hp * ox_cbrt(hp);
       double den = 1.0 + dt * g * n * n * qm / h73;
       s->qx[i] = s->qx[i] / den;
       s->qy[i] = s->qy[i] / den;
