@@ -30,7 +30,8 @@ FIELDS = ("z", "zb", "h", "qx", "qy", "twet", "h0", "fe_1", "fe_2", "fe_3", "fn_
 EXPORTED = ("fx_create", "fx_destroy", "fx_last_error", "fx_device_bytes", "fx_upload", "fx_download",
             "fx_upload_flags", "fx_download_flags", "fx_set_forcing", "fx_set_manning",
             "fx_set_melt_field", "fx_set_option", "fx_prepare", "fx_step", "fx_run_to_print",
-            "fx_print_done", "fx_get_status", "fx_stream", "fx_time_steps", "fx_initiate",
+            "fx_print_done", "fx_get_status", "fx_stream", "fx_time_steps", "fx_adesolver_noalloc",
+            "fx_initiate",
             "fx_load_modset", "fx_open_modset", "fx_write_results", "fx_write_results_host", "fx_run")
 
 
@@ -99,6 +100,7 @@ def lib() -> C.CDLL:
     L.fx_stream.argtypes = [vp]
     L.fx_stream.restype = vp
     L.fx_time_steps.argtypes = [vp, ip, dp, dp, dp]
+    L.fx_adesolver_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, C.c_double, C.c_double, vp]
     L.fx_initiate.argtypes = [vp, dp]
     L.fx_load_modset.argtypes = [cp, C.POINTER(FxGrid), C.POINTER(FxParams), dp, dp, dp, dp, dp, dp,
                                  dp, fp, fp, fp, C.POINTER(ip)]

@@ -1,0 +1,165 @@
+// fx_adesolver_noalloc: one ADE sweep on caller-owned device arrays that
+// allocates no memory at all.
+//
+// Who needs it: callers that are not allowed to call cudaMalloc while they
+// run. Examples are a host model that hands out all of its device memory from
+// its own pool or arena and must stay inside that budget, code that runs
+// while a CUDA graph is being recorded or under a memory-capped job, and
+// coupling layers (the role OpenWQ plays next to FLUXOS) that own the solute
+// arrays and only want the transport step applied to them. Such callers pass
+// device pointers they already hold; this entry point then creates no context,
+// stream or buffer.
+//
+// The sweep needs scratch memory: per strip of 30 rows, the hand-over values
+// of the strip's last row (3 doubles per column) and a progress counter, plus
+// a small control block. Here that scratch is the file-scope device array
+// g_noalloc_scratch of FX_NOALLOC_SCRATCH_BYTES (8 MiB), which every GPU that
+// loads the library holds until the process exits. Grids whose scratch does
+// not fit are rejected (FX_ERR_ARG).
+//
+// On each device, the first call looks up the device address of that array
+// (cudaGetSymbolAddress, with the device current) and the sweep kernel's
+// launch limits; make that first call before any stream capture. Every call
+// shares the one array: calls that overlap on the GPU (other streams, other
+// host threads) race on it and must be serialised by the caller. Each call
+// clears the progress counters and rewrites the control block, the only
+// scratch that must start from a known value.
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "fluxos_gpu.h"
+#include "fx_common.cuh"
+
+void fx_launch_ade(const fx_dev& d, int nstrips, int nblocks, cudaStream_t s);
+int fx_ade_rows_per_strip();
+int fx_ade_threads_per_block();
+int fx_ade_max_blocks(int* out);
+int fx_fail(fx_ctx* ctx, int code, const char* fmt, ...);
+
+#define FX_NOALLOC_SCRATCH_BYTES (8u << 20)
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[FX_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+constexpr size_t kCtlBytes = 256;  // fx_ctl, rounded up
+static_assert(sizeof(fx_ctl) <= kCtlBytes, "control block does not fit its slot");
+
+struct DeviceSetup {
+  bool ready = false;
+  unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
+  int max_blocks = 0;
+};
+DeviceSetup g_setup[kMaxDevices];
+std::mutex g_setup_mutex;
+
+// One sweep with it > 1 (the ADE is skipped on the first solver iteration,
+// ADEsolver_calc.cpp:45) on a fresh epoch.
+__global__ void k_noalloc_ctl(fx_ctl* ctl, double dtfl) {
+  fx_ctl c = {};
+  c.dtfl = dtfl;
+  c.live = 1;
+  c.active = 1;
+  c.it = 2;
+  c.steps = 1;
+  c.stop_after = 1;
+  *ctl = c;
+}
+
+size_t round256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int fx_adesolver_noalloc(double* conc, const double* h, const double* h0, const unsigned char* flags,
+                                    const double* fe_1, const double* fn_1, int nrows, int ncols, int ld, int dxy,
+                                    double dtfl, double d_coef, void* stream) {
+  if (!conc || !h || !h0 || !flags || !fe_1 || !fn_1)
+    return fx_fail(nullptr, FX_ERR_ARG, "fx_adesolver_noalloc: null array");
+  if (nrows < 2 || ncols < 2 || dxy < 1)
+    return fx_fail(nullptr, FX_ERR_ARG, "fx_adesolver_noalloc: need nrows, ncols >= 2 and dxy >= 1");
+  if (ld < nrows + 2 + FX_ROFF || (((long long)ld * (ncols + 2)) & 3) != 0)
+    return fx_fail(nullptr, FX_ERR_ARG,
+                   "fx_adesolver_noalloc: ld must be >= nrows + 3 and ld * (ncols + 2) a multiple of 4");
+  if (((size_t)flags & 3) != 0 || ((size_t)conc & 7) != 0 || ((size_t)h & 7) != 0 || ((size_t)h0 & 7) != 0 ||
+      ((size_t)fe_1 & 7) != 0 || ((size_t)fn_1 & 7) != 0)
+    return fx_fail(nullptr, FX_ERR_ARG, "fx_adesolver_noalloc: misaligned array");
+  if (!(dtfl > 0.0)) return fx_fail(nullptr, FX_ERR_ARG, "fx_adesolver_noalloc: dtfl must be > 0");
+
+  const int rows = fx_ade_rows_per_strip();
+  const int nstrips = (nrows + rows - 1) / rows;
+  const size_t prog_bytes = round256((size_t)nstrips * sizeof(unsigned long long));
+  const size_t bnd_bytes = (size_t)nstrips * (size_t)(ncols + 2) * 3 * sizeof(double);
+  const size_t need = kCtlBytes + prog_bytes + bnd_bytes;
+  if (need > FX_NOALLOC_SCRATCH_BYTES)
+    return fx_fail(nullptr, FX_ERR_ARG,
+                   "fx_adesolver_noalloc: a %d x %d grid needs %zu bytes of scratch, more than the %u-byte "
+                   "static array (use fx_step on a context instead)",
+                   nrows, ncols, need, (unsigned)FX_NOALLOC_SCRATCH_BYTES);
+
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fx_fail(nullptr, FX_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return fx_fail(nullptr, FX_ERR_ARG, "device index %d out of range", dev);
+  {
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    DeviceSetup& s = g_setup[dev];
+    if (!s.ready) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+        return fx_fail(nullptr, FX_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s",
+                       cudaGetErrorString(e));
+      int mb = 0;
+      if (fx_ade_max_blocks(&mb) != 0 || mb < 1)
+        return fx_fail(nullptr, FX_ERR_CUDA, "occupancy query for the ADE sweep failed");
+      s.scratch = (unsigned char*)p;
+      s.max_blocks = mb;
+      s.ready = true;
+    }
+  }
+  const DeviceSetup& s = g_setup[dev];
+  cudaStream_t st = (cudaStream_t)stream;
+
+  fx_dev d;
+  memset(&d, 0, sizeof(d));
+  d.nr = nrows;
+  d.nc = ncols;
+  d.ld = ld;
+  d.nchem = 1;
+  d.plane = (long long)ld * (ncols + 2);
+  d.dxy_u = (unsigned)dxy;
+  d.dxy = (double)dxy;
+  d.arbase = (double)((unsigned long)dxy * (unsigned long)dxy);
+  d.ade = 1;
+  d.dcoef[0] = d_coef;
+  d.conc = conc;
+  d.h = const_cast<double*>(h);
+  d.h0 = const_cast<double*>(h0);
+  d.flags = const_cast<uint8_t*>(flags);
+  d.fe1 = const_cast<double*>(fe_1);
+  d.fn1 = const_cast<double*>(fn_1);
+  d.ctl = reinterpret_cast<fx_ctl*>(s.scratch);
+  d.ade_prog = reinterpret_cast<unsigned long long*>(s.scratch + kCtlBytes);
+  d.ade_bnd = reinterpret_cast<double*>(s.scratch + kCtlBytes + prog_bytes);
+
+  k_noalloc_ctl<<<1, 1, 0, st>>>(d.ctl, dtfl);
+  e = cudaMemsetAsync(d.ade_prog, 0, prog_bytes, st);
+  if (e != cudaSuccess) return fx_fail(nullptr, FX_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+  const int per_block = fx_ade_threads_per_block() / 32;
+  int nblocks = (nstrips + per_block - 1) / per_block;
+  if (nblocks > s.max_blocks) nblocks = s.max_blocks;
+  fx_launch_ade(d, nstrips, nblocks, st);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fx_fail(nullptr, FX_ERR_CUDA, "ADE sweep launch failed: %s", cudaGetErrorString(e));
+  int err = 0;
+  e = cudaMemcpyAsync(&err, &d.ctl->error, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fx_fail(nullptr, FX_ERR_CUDA, "ADE sweep failed: %s", cudaGetErrorString(e));
+  if (err) return fx_fail(nullptr, FX_ERR_DEVICE, "device error %d: a bounded wait in the ADE sweep gave up", err);
+  return FX_OK;
+}

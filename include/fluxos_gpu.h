@@ -125,6 +125,26 @@ void* fx_stream(fx_ctx* ctx);
  * measured launch by launch (for roofline accounting). */
 int fx_time_steps(fx_ctx* ctx, int nsteps, double* ms_total, double* ms_hydro, double* ms_ade);
 
+/* --- allocation-free ADE sweep -------------------------------------------
+ * No counterpart in the reference. For callers that cannot call cudaMalloc
+ * (their device memory comes from their own pool or arena, or they run
+ * inside a fixed memory budget): one ADE step, ADEsolver_calc for one solute
+ * with it > 1, applied in place to `conc` on device arrays the caller owns.
+ * Arrays hold (nrows+2) x (ncols+2) cells; cell (irow, icol) is element
+ * icol*ld + irow + 1 (ld >= nrows+3, ld*(ncols+2) a multiple of 4); `flags`
+ * holds one byte per cell: bit 0 ldry, bit 1 ldry_prev, bit 2 wall. h, h0,
+ * fe_1, fn_1 are the depth after and before the hydrodynamic update and the
+ * face fluxes of that update; dtfl is its time step. The call allocates
+ * nothing: its scratch is one static 8 MiB device array per GPU, so grids
+ * needing more (about 2,900 x 2,900 cells and up) return FX_ERR_ARG. The
+ * first call on a device also looks up that array's device address (do it
+ * before any stream capture). All calls share the array and calls that
+ * overlap on the GPU race. stream NULL = the default stream; the call returns
+ * when the sweep has finished. */
+int fx_adesolver_noalloc(double* conc, const double* h, const double* h0, const unsigned char* flags,
+                         const double* fe_1, const double* fn_1, int nrows, int ncols, int ld, int dxy,
+                         double dtfl, double d_coef, void* stream);
+
 /* --- the reference's file surface (host C++) ---------------------------- */
 /* read_geo's wall/roughness step (read_functions.cpp:175-225) and the zero
  * initial state of initiation (initiate.cpp:43-107,159-228) from the DEM
