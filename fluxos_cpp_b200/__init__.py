@@ -52,7 +52,7 @@ class FxParams(C.Structure):
     _fields_ = [("hdry", C.c_double), ("ks", C.c_double), ("ntim", C.c_double),
                 ("print_step", C.c_double), ("print_next", C.c_double), ("tim", C.c_double),
                 ("h_min_print", C.c_double), ("ade", C.c_int), ("volrat_mode", C.c_int),
-                ("d_coef", C.c_double * MAX_CHEM)]
+                ("d_coef", C.c_double * MAX_CHEM), ("steps_in_flight", C.c_int)]
 
 
 class FxStatus(C.Structure):
@@ -176,7 +176,7 @@ class Domain:
                  xll: float = 0.0, yll: float = 0.0, hdry: float = 0.001, ks: Optional[float] = None,
                  ntim: float = 0.0, print_step: float = 600.0, print_next: Optional[float] = None,
                  tim: float = 0.0, h_min_print: float = 0.0, ade: bool = True, volrat_mode: int = 0,
-                 d_coef: Sequence[float] = (0.01,), _handle=None):
+                 d_coef: Sequence[float] = (0.01,), steps_in_flight: int = 0, _handle=None):
         self.L = lib()
         self.nrows, self.ncols, self.dxy, self.nchem = nrows, ncols, dxy, nchem
         self.xll, self.yll, self.h_min_print = xll, yll, h_min_print
@@ -196,6 +196,7 @@ class Domain:
         p.volrat_mode = volrat_mode
         for k in range(MAX_CHEM):
             p.d_coef[k] = float(d_coef[k] if k < len(d_coef) else d_coef[-1])
+        p.steps_in_flight = int(steps_in_flight)
         h = C.c_void_p()
         _check(self.L.fx_create(C.byref(g), C.byref(p), C.byref(h)))
         self.h = h

@@ -13,15 +13,28 @@
 //     move lane t-1 -> t with one shuffle per step;
 //   * the south carries (updated c, limited flux qfn) stay in registers;
 //   * east / east-east / north / north-north inputs are prefetched by the
-//     owning lane two columns ahead and shuffled down; lanes 30 and 31 only
-//     prefetch the first two rows of the next strip.
+//     owning lane and shuffled down; lanes 30 and 31 only prefetch the first
+//     two rows of the next strip. Prefetches are cp.async copies into a
+//     per-lane shared-memory ring, so no register waits on a load.
 // The re-scale of :47-73 is pointwise, so it is applied to each record as it
 // is loaded; the bounds of :51-62 come from the pre-sweep value of the east
 // and north cells and the re-scaled value of the west and south cells.
-// Strips hand over through a small boundary buffer (per column: updated c,
-// pfe, re-scaled c of the strip's last row) and a release/acquire progress
-// counter; every wait is bounded and sets fx_ctl::error when it gives up.
-// All solutes of the step run in the same launch (independent chains).
+//
+// Steps in flight. The hydrodynamics of a batch of consecutive steps run
+// first (fx_hydro.cu writes each step's depth, fluxes and flags to its own
+// slot plane), then one launch sweeps all of them: step j+1 of a strip
+// follows step j a few diagonals behind, because its inputs are step j's
+// outputs on the same and the next strip. The solute dilution of add_meteo
+// (common.cpp:226-234), the only other writer of the concentration, is
+// applied here, to each record as it is loaded, with the depths before and
+// after the step's melt that the hydrodynamic kernel stored. A single launch therefore holds
+// steps x solutes x strips independent chains and pays the wavefront's
+// start-up once per batch instead of once per step.
+//
+// Strips of one step hand over through a small boundary buffer (per column:
+// updated c, pfe, re-scaled c of the strip's last row); every dependency is a
+// release/acquire progress counter tagged with the step number. Every wait
+// is bounded and sets fx_ctl::error when it gives up.
 #include <cuda_runtime.h>
 
 #include "fx_common.cuh"
@@ -30,18 +43,22 @@ namespace fxade {
 
 constexpr int ROWS = 30;      // rows per strip (lanes 0..29 compute)
 constexpr int WARPS = 4;      // warps per block
-constexpr int CHUNK = 8;      // steps between progress publications
-constexpr int RING = 16;      // per-lane prefetch slots (a power of two)
-constexpr int DIST = 12;      // prefetch distance in columns (< RING)
+constexpr int CHUNK = 4;      // steps between progress checks and publications
+constexpr int RING = 8;       // per-lane prefetch slots (a power of two)
+constexpr int DIST = 4;       // prefetch distance in columns (< RING)
 constexpr long long SPIN_LIMIT = 1LL << 20;  // polls (well under a second) before giving up
 
 // Per-lane ring of prefetched cells, filled by cp.async (asynchronous
-// global -> shared copies: the loads of a future column are in flight while
-// the lane computes, and no register waits on them).
+// global -> shared copies).
 struct Ring {
-  double c[RING][32];    // concentration before the sweep
-  double h0[RING][32];   // depth after forcing, before the update (re-scale)
+  // the 16-byte aligned pair of concentrations holding this lane's cell: it
+  // is written during the launch by other warps, so it is copied with
+  // cp.async.cg (L2 only; L1 is not coherent across SMs), which moves 16 bytes
+  double c[RING][32][2];
+  double h0[RING][32];   // depth after the melt, before the update
   double h[RING][32];    // depth after the update
+  double hp[RING][32];   // depth before the step's melt
+  double mm[RING][32];   // melt-rate multiplier (1 without a melt field)
   double fe1[RING][32];  // fe_1
   double fn1[RING][32];  // fn_1
   unsigned fl[RING][32]; // the 4-byte word holding the cell's flag byte
@@ -56,6 +73,14 @@ struct Rec {
   int ld;     // ldry (1 = dry); ghost cells read 0
 };
 
+// The step a unit works on.
+struct StepIn {
+  long long cur;        // slot plane offset of the step
+  double meteo_rate, meteoi, mconc, dt;
+  bool sweep;           // the sweep runs (hpall != 0 and it > 1)
+  bool dilute;          // add_meteo's dilution runs
+};
+
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
   const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
   const int n = valid ? 8 : 0;  // 0 source bytes: the slot is zero-filled
@@ -66,6 +91,11 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool val
   const int n = valid ? 4 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
 }
+__device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem, bool valid) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {
@@ -73,22 +103,29 @@ __device__ __forceinline__ void cp_wait() {
 }
 
 // Issue the copies of cell (ix, iy) into ring slot `slot` of this lane.
-__device__ __forceinline__ void prefetch(const fx_dev& d, const double* A, Ring& R, int lane, int ix,
-                                         int iy) {
+__device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const double* A, Ring& R, int lane,
+                                         int ix, int iy) {
   const int slot = iy & (RING - 1);
   const bool inr = ix >= 0 && ix <= d.nr + 1 && iy >= 0 && iy <= d.nc + 1;
   const long long gi = inr ? fx_ix(d, ix, iy) : 0;
-  cp_async8(&R.c[slot][lane], A + gi, inr);
-  cp_async8(&R.h0[slot][lane], d.h0 + gi, inr);
-  cp_async8(&R.h[slot][lane], d.h + gi, inr);
-  cp_async8(&R.fe1[slot][lane], d.fe1 + gi, inr);
-  cp_async8(&R.fn1[slot][lane], d.fn1 + gi, inr);
-  cp_async4(&R.fl[slot][lane], d.flags + (gi & ~3LL), inr);
+  cp_async16_cg(&R.c[slot][lane][0], A + (gi & ~1LL), inr);
+  cp_async8(&R.h0[slot][lane], d.h0 + S.cur + gi, inr);
+  cp_async8(&R.h[slot][lane], d.h + S.cur + gi, inr);
+  cp_async8(&R.hp[slot][lane], S.dilute ? (const void*)(d.hpm + S.cur + gi) : (const void*)d.h,
+            inr && S.dilute);
+  const bool mm_ok = inr && S.dilute && d.melt_mult != nullptr;
+  cp_async8(&R.mm[slot][lane], mm_ok ? (const void*)(d.melt_mult + gi) : (const void*)d.h, mm_ok);
+  cp_async8(&R.fe1[slot][lane], d.fe1 + S.cur + gi, inr);
+  cp_async8(&R.fn1[slot][lane], d.fn1 + S.cur + gi, inr);
+  cp_async4(&R.fl[slot][lane], d.flags + S.cur + (gi & ~3LL), inr);
 }
 
-// The record of cell (ix, iy) from its ring slot, re-scaled as
-// ADEsolver_calc.cpp:64-72 does; ghost cells carry only their depth.
-__device__ __forceinline__ Rec make_rec(const fx_dev& d, const Ring& R, int lane, int ix, int iy) {
+// The record of cell (ix, iy) from its ring slot: add_meteo's dilution
+// (common.cpp:214-234) when the step has one, then the re-scale of
+// ADEsolver_calc.cpp:64-72 when the step sweeps. Ghost cells carry only their
+// depth (their concentration is 0 and never changes).
+__device__ __forceinline__ Rec make_rec(const fx_dev& d, const StepIn& S, const Ring& R, int lane, int ix,
+                                        int iy) {
   Rec r;
   r.c = 0.0;
   r.b = 0.0;
@@ -104,9 +141,19 @@ __device__ __forceinline__ Rec make_rec(const fx_dev& d, const Ring& R, int lane
     const unsigned fl = (R.fl[slot][lane] >> (8 * (unsigned)(gi & 3))) & 0xffu;
     r.ld = fl & FX_F_LDRY;
     const int ldp = (fl & FX_F_LDRY_PREV) ? 1 : 0;
-    const double c = R.c[slot][lane];
+    double c = R.c[slot][lane][gi & 1];
+    const double h0 = R.h0[slot][lane];
+    if (S.dilute && !(fl & FX_F_NODATA)) {
+      const double hp = R.hp[slot][lane];
+      if (hp != 0.0) {
+        const double mi =
+            d.melt_mult ? (double)S.meteo_rate * R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt : S.meteoi;
+        c = (c * hp + (mi * S.mconc)) / (h0);
+      }
+    }
     r.c = c;
-    if (r.ld == 0 && ldp == 0) r.b = c * R.h0[slot][lane] / r.h;
+    if (!S.sweep) r.b = c;
+    else if (r.ld == 0 && ldp == 0) r.b = c * h0 / r.h;
     else if (r.ld == 1) r.b = 0.0;
     else r.b = c;
     r.qx = R.fe1[slot][lane];
@@ -136,14 +183,14 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, double D, double dt, b
                                          int ldE, int ldW, int ldEE, int ldN, int ldS, int ldNN,
                                          double cmax, double cmin, double& con, double& pfe_out,
                                          double& qfn_out) {
-  const double nt = 1, sigc = 0.5;
+  const double nt = 1;
   const double dx = d.dxy, dy = d.dxy;
   const double area = d.arbase, areae = d.arbase, arean = d.arbase;
   const double ntp = nt;
   double fem, pfde, hnue, hne;
   if (ldE == 0) {  // :151-172
     hnue = fmax(hp * nt * he * nt, .0001);
-    hne = sqrt(hnue) / sigc / dx * dy * D;
+    hne = fx_div_dxy(d, sqrt(hnue) * 2.0) * dy * D;  // sigc = 0.5: /sigc is *2 exactly
     pfde = -hne * (fe - fp);
     if (qxl > 0.0) {
       if (ldW == 0) fem = -.125 * fw + .75 * fp + .375 * fe;
@@ -171,7 +218,7 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, double D, double dt, b
   double fnm, qfdn, hnn;
   if (ldN == 0) {  // :198-218
     hnue = fmax(.0001, hp * ntp * hn * nt);
-    hnn = sqrt(hnue) / sigc / dy * dx * D;
+    hnn = fx_div_dxy(d, sqrt(hnue) * 2.0) * dx * D;
     qfdn = -hnn * (fn - fp);
     if (qyl > 0.0) {
       if (ldS == 0) fnm = -.125 * fs + .75 * fp + .375 * fn;
@@ -224,7 +271,7 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, double D, double dt, b
       qfn = 0.0;
     }
   }
-  const double dc = (pfw - pfe + qfs - qfn) * dt / area;  // :281-286
+  const double dc = fx_div_area(d, (pfw - pfe + qfs - qfn) * dt);  // :281-286
   double cn = fp + dc / hp;
   cn = fmin(cmax, cn);
   cn = fmax(cmin, cn);
@@ -233,11 +280,13 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, double D, double dt, b
   qfn_out = qfn;
 }
 
-// Wait until strip progress reaches `need` warp steps of this epoch; false
-// if the wait gave up (the error flag is then set).
-__device__ __forceinline__ bool wait_progress(const fx_dev& d, const unsigned long long* prog, unsigned epoch,
-                                              int need) {
-  const unsigned long long want = ((unsigned long long)epoch << 32) | (unsigned)need;
+// Wait until a progress counter reaches `need` warp steps of step `tag`;
+// false if the wait gave up (the error flag is then set). A null counter is
+// no dependency.
+__device__ __forceinline__ bool wait_progress(const fx_dev& d, const unsigned long long* prog,
+                                              unsigned long long tag, int need) {
+  if (!prog) return true;
+  const unsigned long long want = (tag << 32) | (unsigned)need;
   long long it = 0;
   for (;;) {
     const unsigned long long v = ld_acquire(prog);
@@ -253,44 +302,91 @@ __device__ __forceinline__ bool wait_progress(const fx_dev& d, const unsigned lo
 
 __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_nj;
+  __shared__ int s_slot[FX_MAX_SLOTS];
   const fx_ctl& cc = *d.ctl;
-  if (!cc.live || !cc.active || !d.ade || cc.it <= 1) return;  // :45,74-77
-  const double dt = cc.dtfl;
-  const unsigned epoch = (unsigned)cc.steps;
+  if (!d.ade) return;
+  if (threadIdx.x == 0) {
+    // this batch's live steps, in step order
+    int n = 0;
+    for (int k = 0; k < d.nslot; ++k) {
+      const fx_steprec& r = cc.rec[k];
+      if (r.live && r.batch == cc.batch) {
+        int j = n++;
+        while (j > 0 && cc.rec[s_slot[j - 1]].step > r.step) {
+          s_slot[j] = s_slot[j - 1];
+          --j;
+        }
+        s_slot[j] = k;
+      }
+    }
+    s_nj = n;
+  }
+  __syncthreads();
+  const int nj = s_nj;
+  if (nj == 0) return;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   Ring& R = reinterpret_cast<Ring*>(smem_raw)[wib];
   const int wg = blockIdx.x * WARPS + wib;
   const int nwarps = gridDim.x * WARPS;
-  const int units = nstrips * d.nchem;
+  const int per_step = nstrips * d.nchem;
+  const int units = nj * per_step;
   const int T = d.nc + ROWS - 1;  // warp steps per strip
   const long long bnd_stride = (long long)(d.nc + 2) * 3;
+  auto unit_index = [&](int slot, int k, int s) { return ((long long)slot * d.nchem + k) * nstrips + s; };
 
   for (int u = wg; u < units; u += nwarps) {
-    const int k = u / nstrips, s = u % nstrips;
+    const int jj = u / per_step, rem = u % per_step;
+    const int k = rem / nstrips, s = rem % nstrips;
+    const int slot = s_slot[jj];
+    const fx_steprec& rec = cc.rec[slot];
+    const unsigned long long tag = (unsigned long long)rec.step;
+    StepIn S;
+    S.cur = fx_slot(d, rec.step);
+    S.meteo_rate = rec.meteo_rate;
+    S.meteoi = rec.meteoi;
+    S.mconc = rec.mconc;
+    S.dt = rec.dtfl;
+    S.sweep = rec.active && rec.it > 1;  // :45,74-77
+    S.dilute = d.has_meteo != 0;
     double* A = d.conc + k * d.plane;
     const double D = d.dcoef[k];
     const int ix0 = 1 + s * ROWS;
     const int ix = ix0 + lane;
     const bool compute_lane = lane < ROWS && ix <= d.nr;
-    const unsigned long long* prog_prev =
-        (s > 0) ? d.ade_prog + (long long)k * nstrips + (s - 1) : nullptr;
-    unsigned long long* prog_me = d.ade_prog + (long long)k * nstrips + s;
-    const double* bnd_in = d.ade_bnd + ((long long)k * nstrips + s) * bnd_stride;
-    double* bnd_out =
-        (s + 1 < nstrips) ? d.ade_bnd + ((long long)k * nstrips + s + 1) * bnd_stride : nullptr;
+    // dependencies: the west strip of this step, this strip and the next
+    // strip of the previous step of the batch (earlier batches are complete)
+    const unsigned long long* prog_w = (s > 0) ? d.ade_prog + unit_index(slot, k, s - 1) : nullptr;
+    const int pslot = jj > 0 ? s_slot[jj - 1] : -1;
+    const unsigned long long* prog_p0 = jj > 0 ? d.ade_prog + unit_index(pslot, k, s) : nullptr;
+    const unsigned long long* prog_p1 =
+        (jj > 0 && s + 1 < nstrips) ? d.ade_prog + unit_index(pslot, k, s + 1) : nullptr;
+    unsigned long long* prog_me = d.ade_prog + unit_index(slot, k, s);
+    const double* bnd_in = d.ade_bnd + unit_index(slot, k, s) * bnd_stride;
+    double* bnd_out = (s + 1 < nstrips) ? d.ade_bnd + unit_index(slot, k, s + 1) * bnd_stride : nullptr;
+    bool bail = false;
+
+    // the previous step must have written every column prefetched before a
+    // check: lanes 0..29 of its strip s, lanes 0..1 of its strip s + 1
+    auto prev_ready = [&](int col) {
+      return wait_progress(d, prog_p0, tag - 1, min(col + ROWS, T)) &&
+             wait_progress(d, prog_p1, tag - 1, min(col + 2, T));
+    };
+    if (!prev_ready(DIST + 3)) bail = true;
 
     // prime the ring: columns iy0 .. iy0 + DIST + 2 of this lane's row
     const int iy0 = 1 - lane;
-    __syncwarp();
-    for (int j = 0; j < DIST + 3; ++j) {
-      prefetch(d, A, R, lane, ix, iy0 + j);
-      cp_commit();
+    if (!bail) {
+      for (int j = 0; j < DIST + 3; ++j) {
+        prefetch(d, S, A, R, lane, ix, iy0 + j);
+        cp_commit();
+      }
     }
     cp_wait<0>();
-    Rec cur = make_rec(d, R, lane, ix, iy0);
-    Rec n1 = make_rec(d, R, lane, ix, iy0 + 1);
-    Rec n2 = make_rec(d, R, lane, ix, iy0 + 2);
+    Rec cur = make_rec(d, S, R, lane, ix, iy0);
+    Rec n1 = make_rec(d, S, R, lane, ix, iy0 + 1);
+    Rec n2 = make_rec(d, S, R, lane, ix, iy0 + 2);
     // carries: outputs of this lane's previous cell (its south cell for the
     // next step, its west cell for lane + 1)
     double o_c = 0.0, o_pfe = 0.0, o_b = 0.0, o_qfn = 0.0;
@@ -300,9 +396,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
     // c = 0, pfe = the ghost convective flux c(0,iy)*fe_1(0,iy)*dy = 0 (:106-116)
     double bw_c = 0.0, bw_pfe = 0.0, bw_b = 0.0, bn_c = 0.0, bn_pfe = 0.0, bn_b = 0.0;
     int bw_ld = 0, bn_ld = 0;
-    bool bail = false;
-    if (prog_prev) {
-      if (!wait_progress(d, prog_prev, epoch, min(CHUNK - 1 + ROWS, T))) {
+    if (!bail && prog_w) {
+      if (!wait_progress(d, prog_w, tag, min(CHUNK - 1 + ROWS, T))) {
         bail = true;
       } else {
         const int iyb = 1 + lane;
@@ -311,7 +406,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
           bn_c = __ldcg(p);
           bn_pfe = __ldcg(p + 1);
           bn_b = __ldcg(p + 2);
-          bn_ld = d.flags[fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
+          bn_ld = d.flags[S.cur + fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
         }
       }
     }
@@ -322,9 +417,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
         bw_pfe = bn_pfe;
         bw_b = bn_b;
         bw_ld = bn_ld;
-        if (prog_prev && tau + CHUNK < T) {
+        // columns lane 0 prefetches during this chunk
+        if (!prev_ready(tau + CHUNK + DIST + 3)) {
+          bail = true;
+          break;
+        }
+        if (prog_w && tau + CHUNK < T) {
           // the next chunk's boundary: wait for it now, use it in CHUNK steps
-          if (!wait_progress(d, prog_prev, epoch, min(tau + 2 * CHUNK - 1 + ROWS, T))) {
+          if (!wait_progress(d, prog_w, tag, min(tau + 2 * CHUNK - 1 + ROWS, T))) {
             bail = true;
             break;
           }
@@ -336,14 +436,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
             bn_c = __ldcg(p);
             bn_pfe = __ldcg(p + 1);
             bn_b = __ldcg(p + 2);
-            bn_ld = d.flags[fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
+            bn_ld = d.flags[S.cur + fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
           }
         }
       }
       const int iy = tau - lane + 1;
       // keep DIST columns in flight: column iy + DIST + 3 now, column iy + 3
       // must have landed by the end of this step
-      prefetch(d, A, R, lane, ix, iy + DIST + 3);
+      prefetch(d, S, A, R, lane, ix, iy + DIST + 3);
       cp_commit();
       // east (lane+1's next column), east-east (lane+2's column after next)
       const double E_c = shdn(n1.c, 1), E_b = shdn(n1.b, 1), E_h = shdn(n1.h, 1);
@@ -374,14 +474,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
         }
         const double NN_b = last_col ? n1.b : n2.b;  // inn = min(iy+2, NCOLS+1)
         const int NN_ld = last_col ? n1.ld : n2.ld;
-        if (last_row && last_col) {
-          out_c = cur.b;  // the sweep stops one cell short (:93)
+        if (!S.sweep || (last_row && last_col)) {
+          out_c = cur.b;  // no sweep this step, or the cell the sweep stops short of (:93)
         } else if (cur.ld == 1) {
           out_c = 0.0;  // :119-124
         } else {
           const double cmax = fmax(W_b, fmax(E_c, fmax(o_b, n1.c)));
           const double cmin = fmin(W_b, fmin(E_c, fmin(o_b, n1.c)));
-          ade_cell(d, D, dt, last_row, last_col, cur.h, E_h, n1.h, cur.qx, cur.qy, W_c, cur.b, E_b,
+          ade_cell(d, D, S.dt, last_row, last_col, cur.h, E_h, n1.h, cur.qx, cur.qy, W_c, cur.b, E_b,
                    EE_b, o_c, n1.b, NN_b, W_pfe, o_qfn, E_ld, W_ld, EE_ld, n1.ld, o_ld, NN_ld, cmax,
                    cmin, out_c, pfe, qfn);
         }
@@ -405,17 +505,20 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
         o_ld = 0;
         o_qfn = 0.0;
       }
-      // publish progress (lane 29 owns the boundary values)
+      // publish progress: every lane's writes of this chunk, then the count.
+      // The next strip of this step overwrites its first two rows only after
+      // this count passes the column by ROWS steps; lanes 30 and 31 copied
+      // those rows DIST + 3 columns ahead, and cp_wait below retires a copy
+      // DIST steps after it was issued, so the copies have landed by then.
       if (((tau + 1) % CHUNK) == 0 || tau + 1 == T) {
-        if (lane == ROWS - 1) {
-          __threadfence();
-          st_release(prog_me, ((unsigned long long)epoch << 32) | (unsigned)(tau + 1));
-        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release(prog_me, (tag << 32) | (unsigned)(tau + 1));
       }
       cp_wait<DIST>();
       cur = n1;
       n1 = n2;
-      n2 = make_rec(d, R, lane, ix, iy + 3);
+      n2 = make_rec(d, S, R, lane, ix, iy + 3);
     }
     cp_wait<0>();
     if (bail) return;

@@ -15,6 +15,8 @@
 #include "fx_internal.h"
 
 void fx_launch_finalize(const fx_dev& d, cudaStream_t s);
+void fx_launch_batch_begin(const fx_dev& d, cudaStream_t s);
+void fx_launch_mark_static(const fx_dev& d, cudaStream_t s);
 void fx_launch_hydro(const fx_dev& d, cudaStream_t s);
 void fx_launch_courant_scan(const fx_dev& d, cudaStream_t s);
 void fx_launch_ade(const fx_dev& d, int nstrips, int nblocks, cudaStream_t s);
@@ -25,7 +27,6 @@ int fx_ade_max_blocks(int* out);
 static thread_local std::string g_last_error;
 
 static const unsigned long long kInfBits = 0x7ff0000000000000ull;
-static const int kGraphSteps = 16;
 
 int fx_fail(fx_ctx* ctx, int code, const char* fmt, ...) {
   char buf[512];
@@ -45,6 +46,12 @@ int fx_fail(fx_ctx* ctx, int code, const char* fmt, ...) {
       return fx_fail(ctx, e_ == cudaErrorMemoryAllocation ? FX_ERR_NOMEM : FX_ERR_CUDA,    \
                      "%s failed: %s", #call, cudaGetErrorString(e_));                      \
   } while (0)
+
+// Fields with one plane per slot (the state after step n lives in plane
+// n % nslot); the others have a single plane.
+static bool slot_field(const char* name) {
+  return !strcmp(name, "h") || !strcmp(name, "h0") || !strcmp(name, "fe_1") || !strcmp(name, "fn_1");
+}
 
 static double* field_ptr(fx_ctx* c, const char* name) {
   fx_dev& d = c->d;
@@ -133,9 +140,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
   d.nchem = g->nchem;
   d.ld = ((g->nrows + 2 + FX_ROFF + 31) / 32) * 32;
   d.plane = (long long)d.ld * (g->ncols + 2);
-  d.dxy_u = (unsigned)g->dxy;
-  d.dxy = (double)g->dxy;
-  d.arbase = (double)((unsigned long)g->dxy * (unsigned long)g->dxy);
+  fx_set_cell_size(d, g->dxy);
   d.hdry = p->hdry;
   d.ks = p->ks;
   d.nodata = g->nodata;
@@ -148,14 +153,22 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
   d.volrat_mode = p->volrat_mode;
   d.ade = p->ade;
   for (int k = 0; k < FX_MAX_CHEM; ++k) d.dcoef[k] = p->d_coef[k];
+  {
+    int k = p->steps_in_flight > 0 ? p->steps_in_flight : 8;
+    if (k > FX_MAX_SLOTS - 1) k = FX_MAX_SLOTS - 1;
+    d.nslot = k + 1;  // a batch of k steps plus the state before it
+    c->batch_steps = k;
+  }
   const size_t pb = (size_t)d.plane * sizeof(double);
   int rc = FX_OK;
-  double** fields[] = {&d.z, &d.zb, &d.h, &d.qx, &d.qy, &d.twet, &d.h0,
-                       &d.fe1, &d.fe2, &d.fe3, &d.fn1, &d.fn2, &d.fn3};
+  double** fields[] = {&d.z, &d.zb, &d.qx, &d.qy, &d.twet, &d.fe2, &d.fe3, &d.fn2, &d.fn3};
+  double** slot_fields[] = {&d.h, &d.h0, &d.hpm, &d.fe1, &d.fn1};
   for (double** f : fields)
     if ((rc = dev_alloc(c, (void**)f, pb)) != FX_OK) goto fail;
+  for (double** f : slot_fields)
+    if ((rc = dev_alloc(c, (void**)f, pb * d.nslot)) != FX_OK) goto fail;
   if ((rc = dev_alloc(c, (void**)&d.conc, pb * g->nchem)) != FX_OK) goto fail;
-  if ((rc = dev_alloc(c, (void**)&d.flags, (size_t)d.plane)) != FX_OK) goto fail;
+  if ((rc = dev_alloc(c, (void**)&d.flags, (size_t)d.plane * d.nslot)) != FX_OK) goto fail;
   if ((rc = dev_alloc(c, (void**)&d.ctl, sizeof(fx_ctl))) != FX_OK) goto fail;
   {
     float* tab = nullptr;
@@ -166,10 +179,10 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
   }
   c->ade_strips = (g->nrows + fx_ade_rows_per_strip() - 1) / fx_ade_rows_per_strip();
   if ((rc = dev_alloc(c, (void**)&d.ade_bnd,
-                      sizeof(double) * (size_t)g->nchem * c->ade_strips * (g->ncols + 2) * 3)) != FX_OK)
+                      sizeof(double) * (size_t)d.nslot * g->nchem * c->ade_strips * (g->ncols + 2) * 3)) != FX_OK)
     goto fail;
-  if ((rc = dev_alloc(c, (void**)&d.ade_prog, sizeof(unsigned long long) * (size_t)g->nchem * c->ade_strips)) !=
-      FX_OK)
+  if ((rc = dev_alloc(c, (void**)&d.ade_prog,
+                      sizeof(unsigned long long) * (size_t)d.nslot * g->nchem * c->ade_strips)) != FX_OK)
     goto fail;
   {
     int maxb = 0;
@@ -177,7 +190,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
       rc = fx_fail(c, FX_ERR_CUDA, "occupancy query for the ADE sweep failed");
       goto fail;
     }
-    const int units = g->nchem * c->ade_strips;
+    const int units = c->batch_steps * g->nchem * c->ade_strips;
     const int per_block = fx_ade_threads_per_block() / 32;
     int want = (units + per_block - 1) / per_block;
     c->ade_blocks = want < maxb ? want : maxb;
@@ -230,8 +243,11 @@ int fx_upload(fx_ctx* c, const char* field, const double* host) {
   double* dst = field_ptr(c, field);
   if (!dst) return fx_fail(c, FX_ERR_ARG, "fx_upload: unknown field '%s'", field);
   const int mr = c->d.nr + 2, mc = c->d.nc + 2;
-  FX_CK(c, cudaMemcpy2DAsync(dst + FX_ROFF, (size_t)c->d.ld * sizeof(double), host, (size_t)mr * sizeof(double),
-                             (size_t)mr * sizeof(double), (size_t)mc, cudaMemcpyHostToDevice, c->stream));
+  const int planes = slot_field(field) ? c->d.nslot : 1;  // every slot holds the uploaded state
+  for (int k = 0; k < planes; ++k)
+    FX_CK(c, cudaMemcpy2DAsync(dst + k * c->d.plane + FX_ROFF, (size_t)c->d.ld * sizeof(double), host,
+                               (size_t)mr * sizeof(double), (size_t)mr * sizeof(double), (size_t)mc,
+                               cudaMemcpyHostToDevice, c->stream));
   FX_CK(c, cudaStreamSynchronize(c->stream));
   c->prepared = false;
   return FX_OK;
@@ -241,6 +257,11 @@ int fx_download(fx_ctx* c, const char* field, double* host) {
   if (!c || !field || !host) return fx_fail(c, FX_ERR_ARG, "fx_download: null argument");
   double* src = field_ptr(c, field);
   if (!src) return fx_fail(c, FX_ERR_ARG, "fx_download: unknown field '%s'", field);
+  if (slot_field(field)) {
+    int rc = read_ctl(c);
+    if (rc) return rc;
+    src += fx_slot(c->d, c->ctl_host->steps);
+  }
   const int mr = c->d.nr + 2, mc = c->d.nc + 2;
   FX_CK(c, cudaMemcpy2DAsync(host, (size_t)mr * sizeof(double), src + FX_ROFF, (size_t)c->d.ld * sizeof(double),
                              (size_t)mr * sizeof(double), (size_t)mc, cudaMemcpyDeviceToHost, c->stream));
@@ -254,8 +275,9 @@ int fx_upload_flags(fx_ctx* c, const float* ldry, const float* wall) {
   std::vector<uint8_t> fl((size_t)mr * mc);
   for (size_t i = 0; i < fl.size(); ++i)
     fl[i] = (uint8_t)((ldry[i] == 1.0f ? FX_F_LDRY : 0) | (wall[i] == 1.0f ? FX_F_WALL : 0));
-  FX_CK(c, cudaMemcpy2DAsync(c->d.flags + FX_ROFF, (size_t)c->d.ld, fl.data(), (size_t)mr, (size_t)mr, (size_t)mc,
-                             cudaMemcpyHostToDevice, c->stream));
+  for (int k = 0; k < c->d.nslot; ++k)
+    FX_CK(c, cudaMemcpy2DAsync(c->d.flags + k * c->d.plane + FX_ROFF, (size_t)c->d.ld, fl.data(), (size_t)mr,
+                               (size_t)mr, (size_t)mc, cudaMemcpyHostToDevice, c->stream));
   FX_CK(c, cudaStreamSynchronize(c->stream));
   c->prepared = false;
   return FX_OK;
@@ -265,8 +287,10 @@ int fx_download_flags(fx_ctx* c, float* ldry, float* ldry_prev, float* wall) {
   if (!c) return FX_ERR_ARG;
   const int mr = c->d.nr + 2, mc = c->d.nc + 2;
   std::vector<uint8_t> fl((size_t)mr * mc);
-  FX_CK(c, cudaMemcpy2DAsync(fl.data(), (size_t)mr, c->d.flags + FX_ROFF, (size_t)c->d.ld, (size_t)mr, (size_t)mc,
-                             cudaMemcpyDeviceToHost, c->stream));
+  int rc = read_ctl(c);
+  if (rc) return rc;
+  FX_CK(c, cudaMemcpy2DAsync(fl.data(), (size_t)mr, c->d.flags + fx_slot(c->d, c->ctl_host->steps) + FX_ROFF,
+                             (size_t)c->d.ld, (size_t)mr, (size_t)mc, cudaMemcpyDeviceToHost, c->stream));
   FX_CK(c, cudaStreamSynchronize(c->stream));
   for (size_t i = 0; i < fl.size(); ++i) {
     if (ldry) ldry[i] = (fl[i] & FX_F_LDRY) ? 1.0f : 0.0f;
@@ -343,6 +367,7 @@ int fx_prepare(fx_ctx* c) {
   c->ctl_host->acc_dtmin = kInfBits;
   c->ctl_host->acc_hmax = 0ull;
   FX_CK(c, cudaMemcpyAsync(c->d.ctl, c->ctl_host, sizeof(fx_ctl), cudaMemcpyHostToDevice, c->stream));
+  fx_launch_mark_static(c->d, c->stream);
   fx_launch_courant_scan(c->d, c->stream);
   FX_CK(c, cudaGetLastError());
   FX_CK(c, cudaStreamSynchronize(c->stream));
@@ -352,9 +377,14 @@ int fx_prepare(fx_ctx* c) {
 
 }  // extern "C"
 
-static void launch_step(fx_ctx* c) {
-  fx_launch_finalize(c->d, c->stream);
-  fx_launch_hydro(c->d, c->stream);
+// One batch of m steps: the clock and the hydrodynamics step by step, then
+// the ADE sweeps of all m steps in one launch (fx_ade.cu).
+static void launch_batch(fx_ctx* c, int m) {
+  fx_launch_batch_begin(c->d, c->stream);
+  for (int i = 0; i < m; ++i) {
+    fx_launch_finalize(c->d, c->stream);
+    fx_launch_hydro(c->d, c->stream);
+  }
   fx_launch_ade(c->d, c->ade_strips, c->ade_blocks, c->stream);
 }
 
@@ -366,7 +396,7 @@ static int ensure_graph(fx_ctx* c) {
   }
   cudaGraph_t graph = nullptr;
   FX_CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < kGraphSteps; ++i) launch_step(c);
+  launch_batch(c, c->batch_steps);
   FX_CK(c, cudaStreamEndCapture(c->stream, &graph));
   cudaError_t e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
   cudaGraphDestroy(graph);
@@ -402,11 +432,11 @@ int fx_step(fx_ctx* c, int nsteps, fx_status* st) {
   if ((rc = set_stop(c, c->ctl_host->steps + nsteps))) return rc;
   if ((rc = ensure_graph(c))) return rc;
   int left = nsteps;
-  while (left >= kGraphSteps) {
+  while (left >= c->batch_steps) {
     FX_CK(c, cudaGraphLaunch(c->graph_exec, c->stream));
-    left -= kGraphSteps;
+    left -= c->batch_steps;
   }
-  for (int i = 0; i < left; ++i) launch_step(c);
+  if (left > 0) launch_batch(c, left);
   FX_CK(c, cudaGetLastError());
   if ((rc = read_ctl(c))) return rc;
   fill_status(*c->ctl_host, st);
@@ -423,7 +453,7 @@ int fx_run_to_print(fx_ctx* c, fx_status* st) {
     // Enough steps to reach the next output at the current dt, within limits.
     double est = (k.dtfl > 0 && std::isfinite(k.dtfl)) ? (k.print_next - k.tim) / k.dtfl : 16.0;
     long long n = (long long)std::ceil(est) + 2;
-    if (n < kGraphSteps) n = kGraphSteps;
+    if (n < c->batch_steps) n = c->batch_steps;
     if (n > 4096) n = 4096;
     rc = fx_step(c, (int)n, nullptr);
     if (rc) return rc;
@@ -462,28 +492,56 @@ int fx_time_steps(fx_ctx* c, int n, double* ms_total, double* ms_hydro, double* 
   int rc = read_ctl(c);
   if (rc) return rc;
   if ((rc = set_stop(c, c->ctl_host->steps + n))) return rc;
-  std::vector<cudaEvent_t> ev(3 * (size_t)n + 1);
-  for (auto& e : ev) FX_CK(c, cudaEventCreate(&e));
-  FX_CK(c, cudaEventRecord(ev[0], c->stream));
-  for (int i = 0; i < n; ++i) {
-    fx_launch_finalize(c->d, c->stream);
-    FX_CK(c, cudaEventRecord(ev[3 * i + 1], c->stream));
-    fx_launch_hydro(c->d, c->stream);
-    FX_CK(c, cudaEventRecord(ev[3 * i + 2], c->stream));
+  // events: the start, then per step: after its clock update and after its
+  // hydro launch, and per batch: after the sweep
+  std::vector<cudaEvent_t> ev;
+  ev.reserve(4 + 4 * (size_t)n);
+  auto record = [&](size_t* idx) -> int {
+    cudaEvent_t e = nullptr;
+    FX_CK(c, cudaEventCreate(&e));
+    ev.push_back(e);
+    FX_CK(c, cudaEventRecord(e, c->stream));
+    *idx = ev.size() - 1;
+    return FX_OK;
+  };
+  size_t e_start = 0, a = 0, b = 0;
+  std::vector<std::pair<size_t, size_t>> hyd, ade;
+  int erc = record(&e_start);
+  const int K = c->batch_steps;
+  for (int left = n; left > 0 && !erc;) {
+    const int m = left < K ? left : K;
+    left -= m;
+    fx_launch_batch_begin(c->d, c->stream);
+    for (int i = 0; i < m && !erc; ++i) {
+      fx_launch_finalize(c->d, c->stream);
+      if ((erc = record(&a))) break;
+      fx_launch_hydro(c->d, c->stream);
+      if ((erc = record(&b))) break;
+      hyd.push_back({a, b});
+    }
+    if (erc) break;
+    a = b;
     fx_launch_ade(c->d, c->ade_strips, c->ade_blocks, c->stream);
-    FX_CK(c, cudaEventRecord(ev[3 * i + 3], c->stream));
+    if ((erc = record(&b))) break;
+    ade.push_back({a, b});
+  }
+  if (erc) {
+    for (auto& e : ev) cudaEventDestroy(e);
+    return erc;
   }
   FX_CK(c, cudaGetLastError());
   FX_CK(c, cudaStreamSynchronize(c->stream));
   double th = 0, ta = 0;
   float ms = 0;
-  for (int i = 0; i < n; ++i) {
-    FX_CK(c, cudaEventElapsedTime(&ms, ev[3 * i + 1], ev[3 * i + 2]));
+  for (auto& pr : hyd) {
+    FX_CK(c, cudaEventElapsedTime(&ms, ev[pr.first], ev[pr.second]));
     th += ms;
-    FX_CK(c, cudaEventElapsedTime(&ms, ev[3 * i + 2], ev[3 * i + 3]));
+  }
+  for (auto& pr : ade) {
+    FX_CK(c, cudaEventElapsedTime(&ms, ev[pr.first], ev[pr.second]));
     ta += ms;
   }
-  FX_CK(c, cudaEventElapsedTime(&ms, ev[0], ev[3 * (size_t)n]));
+  FX_CK(c, cudaEventElapsedTime(&ms, ev[e_start], ev.back()));
   for (auto& e : ev) cudaEventDestroy(e);
   if (ms_total) *ms_total = ms;
   if (ms_hydro) *ms_hydro = th;

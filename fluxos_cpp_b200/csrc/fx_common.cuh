@@ -14,14 +14,32 @@
 #define FX_ROFF 1
 #define FX_MAX_CHEM 8
 #define FX_METEO_ROWS 2000
+#define FX_MAX_SLOTS 16
 
 // Per-cell flag byte.
 #define FX_F_LDRY 0x01       // ldry (1 = dry) at the end of the last step
 #define FX_F_LDRY_PREV 0x02  // ldry_prev of the last step (ADE rescale)
 #define FX_F_WALL 0x04       // innerNeumannBCWeir (NODATA or 0 DEM cell)
+#define FX_F_NODATA 0x08     // zb == NODATA_VALUE: add_meteo skips the cell (common.cpp:214)
 
 // Device error codes (fx_ctl::error).
 #define FX_DEVERR_WAIT_TIMEOUT 1
+
+// What the ADE sweep of one step needs besides the grids: written by
+// k_finalize when the step starts, read by the sweep of the same step, which
+// may run several steps later (the hydrodynamics run ahead, see fx_ade.cu).
+struct fx_steprec {
+  double dtfl;        // dt of the step
+  double meteoi;      // uniform melt depth of the step
+  double meteo_rate;  // forcing rate of the step's row [mm/day]
+  double mconc;       // forcing concentration of the step's row
+  long long step;     // absolute step number (1 = first step)
+  long long batch;    // value of fx_ctl::batch when the step ran
+  int live;           // the step ran
+  int active;         // hpall != 0: the hydrodynamic update and the sweep ran
+  int it;             // solver iteration count after the step
+  int pad_;
+};
 
 // Step control block, resident in device memory. One thread of k_finalize
 // advances the clock exactly as main.cpp:271-325 does; every other kernel of
@@ -48,6 +66,8 @@ struct fx_ctl {
   int forcing_overrun;   // the forcing table had no row with t > tim
   int error;             // FX_DEVERR_* set by a kernel
   int pad_;
+  long long batch;       // counts launch batches; the ADE sweep takes this batch's steps
+  fx_steprec rec[FX_MAX_SLOTS];  // per-slot record of the last steps
 };
 
 // Everything a kernel needs, passed by value.
@@ -64,13 +84,21 @@ struct fx_dev {
   double nueml;       // (double)(float)1.793e-6 (main.cpp:135)
   double cvdefl;      // (double)(float)0.07 (main.cpp:134)
   double cfl_dxy;     // (double)((float)cfl * (float)dxy) (main.cpp:316)
+  int dxy_pow2;       // 1 when dxy is a power of two (then x/dxy == x*inv_dxy exactly)
+  double inv_dxy;     // 1/dxy, exact when dxy_pow2
+  double inv_area;    // 1/arbase, exact when dxy_pow2
   int volrat_mode;    // 0: edge flux = weir formula, 1: edge flux = 0
   int ade;            // ADE module on
   int store_all_fluxes;  // 1 when forcing can remove water (see k_hydro)
   int pad_;
   double dcoef[FX_MAX_CHEM];
-  // state
+  // state. h, h0, fe1, fn1 and flags hold `nslot` planes each: the state
+  // after step n lives in plane n % nslot, so the ADE sweep of a step can run
+  // after the hydrodynamics of the following steps (fx_ade.cu).
+  int nslot;
+  int pad3_;
   double *z, *zb, *h, *qx, *qy, *twet, *h0;
+  double* hpm;        // per slot: the depth before the step's melt, max(z - zb, 0) (common.cpp:216)
   double *fe1, *fe2, *fe3, *fn1, *fn2, *fn3;
   double* conc;       // nchem planes of ld*(nc+2)
   uint8_t* flags;
@@ -85,11 +113,35 @@ struct fx_dev {
   int pad2_;
   fx_ctl* ctl;
   // ADE sweep scratch
-  double* ade_bnd;                 // per solute, per strip: (ncols+2) x 3
-  unsigned long long* ade_prog;    // per solute, per strip: epoch<<32 | steps done
+  double* ade_bnd;                 // per slot, solute, strip: (ncols+2) x 3
+  unsigned long long* ade_prog;    // per slot, solute, strip: step<<32 | warp steps done
   long long plane;                 // elements per field = ld * (nc + 2)
 };
 
+// x / dxy and x / dxy^2. When dxy is a power of two the quotient is an
+// exact scaling, so multiplying by the exact reciprocal gives the same bits as
+// the division and saves a multi-instruction FP64 divide.
+__host__ __device__ inline double fx_div_dxy(const fx_dev& d, double x) {
+  return d.dxy_pow2 ? x * d.inv_dxy : x / d.dxy;
+}
+__host__ __device__ inline double fx_div_area(const fx_dev& d, double x) {
+  return d.dxy_pow2 ? x * d.inv_area : x / d.arbase;
+}
+
+inline void fx_set_cell_size(fx_dev& d, int dxy) {
+  d.dxy_u = (unsigned)dxy;
+  d.dxy = (double)dxy;
+  d.arbase = (double)((unsigned long)dxy * (unsigned long)dxy);
+  d.dxy_pow2 = dxy > 0 && (dxy & (dxy - 1)) == 0 && dxy <= (1 << 20);
+  d.inv_dxy = 1.0 / d.dxy;
+  d.inv_area = 1.0 / d.arbase;
+}
+
 __host__ __device__ inline long long fx_ix(const fx_dev& d, int irow, int icol) {
   return (long long)icol * d.ld + irow + FX_ROFF;
+}
+
+// Offset of the slot plane that holds the state after step n.
+__host__ __device__ inline long long fx_slot(const fx_dev& d, long long step) {
+  return (step % d.nslot) * d.plane;
 }

@@ -24,11 +24,17 @@
 
 namespace fx {
 
-constexpr int TX = 32, TY = 8;                 // tile: 32 rows (irow) x 8 columns (icol)
+// A block of 32 x 8 threads owns a tile of 31 rows (irow) x 7 columns (icol):
+// with its west row and south column of halo faces the tile has exactly
+// 32 x 8 = 256 face-flux cells, one per thread, so the flux phase runs in a
+// single wave and no warp waits at the barrier for a second round.
+constexpr int BX = 32, BY = 8;                  // threads
+constexpr int TX = 31, TY = 7;                  // owned cells
 constexpr int SX = TX + 3, SY = TY + 3;        // stencil: rows irow0-2..irow0+TX, cols icol0-2..icol0+TY
 constexpr int FXN = TX + 1, FYN = TY + 1;      // fluxes: rows irow0-1..irow0+TX-1, cols icol0-1..icol0+TY-1
 constexpr int NSTEN = SX * SY, NFLUX = FXN * FYN;
-constexpr int NTHREADS = TX * TY;
+constexpr int NTHREADS = BX * BY;
+static_assert(NFLUX == NTHREADS, "one face-flux cell per thread");
 
 // stencil cell classes
 constexpr unsigned char C_DRY = 1;   // Loop-1 ldry == 1 (interior cells only)
@@ -199,8 +205,8 @@ __device__ void solver_wet(const fx_dev& d, const HydroSmem& S, int sr, int sc, 
   const double vwn = S.qy[WN] / fmax(fmax(hat(WN), hdryl), ksat(WN));
   const double ven = S.qy[EN] / fmax(fmax(hat(EN), hdryl), ksat(EN));
 
-  const double txye = hne * ((ve - vp) / fabs((double)dx) + .25 * (un + une - us0 - use0) / dy);
-  const double txyn = hnn * ((un - up) / fabs((double)dy) + .25 * (ve + ven - vw - vwn) / dx);
+  const double txye = hne * (fx_div_dxy(d, ve - vp) + fx_div_dxy(d, .25 * (un + une - us0 - use0)));
+  const double txyn = hnn * (fx_div_dxy(d, un - up) + fx_div_dxy(d, .25 * (ve + ven - vw - vwn)));
 
   const double fe1c = qme;
   const double fe2c = qme * ume;
@@ -283,13 +289,13 @@ __device__ void solver_wet(const fx_dev& d, const HydroSmem& S, int sr, int sc, 
     if (fe1 > 0.0 && fn1 > 0.0) {
       if (fe1 * dy + fn1 * dx > volrat) {
         double cf = fn1 * dx / (fe1 * dy + fn1 * dx);
-        fe1 = (1. - cf) * volrat / dy;
-        fn1 = cf * volrat / dx;
+        fe1 = fx_div_dxy(d, (1. - cf) * volrat);
+        fn1 = fx_div_dxy(d, cf * volrat);
       }
     } else if (fe1 > 0.0) {
-      fe1 = fmin(fe1 * dy, volrat) / dy;
+      fe1 = fx_div_dxy(d, fmin(fe1 * dy, volrat));
     } else if (fn1 > 0.0) {
-      fn1 = fmin(fn1 * dx, volrat) / dx;
+      fn1 = fx_div_dxy(d, fmin(fn1 * dx, volrat));
     }
   } else {
     fe1 = 0.0;
@@ -422,40 +428,44 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
   const fx_ctl c = *d.ctl;
   if (!c.live) return;
   const int lx = threadIdx.x, ly = threadIdx.y;
-  const int tid = ly * TX + lx;
+  const int tid = ly * BX + lx;
   const int irow0 = 1 + blockIdx.x * TX, icol0 = 1 + blockIdx.y * TY;
   const int irow = irow0 + lx, icol = icol0 + ly;
-  const bool own = irow <= d.nr && icol <= d.nc;
+  const bool own = lx < TX && ly < TY && irow <= d.nr && icol <= d.nc;
   const double dtl = c.dtfl;
   const bool melt_on = d.has_meteo != 0;
 
+  // Slot planes: the state after the previous step, and the one this step
+  // writes (h, h0, fe_1, fn_1, flags; see fx_common.cuh).
+  const long long sprev = fx_slot(d, c.steps - 1), scur = fx_slot(d, c.steps);
+
   if (!c.active) {
     // No wet cell: the step is the Courant scan plus add_meteo only
-    // (main.cpp:300-370, the solver block at :385 is skipped).
+    // (main.cpp:300-370, the solver block at :385 is skipped). The solute
+    // dilution of add_meteo is applied by the ADE sweep (fx_ade.cu).
     double dtc = __longlong_as_double(0x7ff0000000000000LL), hm = 0.0;
     if (own) {
       const long long gi = fx_ix(d, irow, icol);
       const double zb = d.zb[gi], zpre = d.z[gi];
-      const uint8_t fl = d.flags[gi];
+      const uint8_t fl = d.flags[sprev + gi];
       const double hpre = fmax(0.0, zpre - zb);
       uint8_t ld = hpre > d.hdry ? 0 : 1;  // Courant scan (:308-320)
       double z1 = zpre, h1 = hpre;
       if (melt_on && zb != d.nodata) {
         const double mi = melt_depth(d, c, gi);
-        const double hp = fmax(zpre - zb, 0.0);
+        if (d.ade) d.hpm[scur + gi] = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
         z1 = zpre + mi;
         h1 = fmax(z1 - zb, 0.0);
         if (h1 <= d.hdry) ld = 0;  // common.cpp:219-222
-        if (d.ade && hp != 0.0)
-          for (int k = 0; k < d.nchem; ++k) {
-            double* cp = d.conc + k * d.plane + gi;
-            *cp = (*cp * hp + (mi * c.mconc)) / (h1);
-          }
         d.z[gi] = z1;
       }
-      d.h[gi] = h1;
-      d.h0[gi] = h1;
-      d.flags[gi] = (fl & FX_F_WALL) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+      d.h[scur + gi] = h1;
+      d.h0[scur + gi] = h1;
+      d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+      if (scur != sprev) {  // fluxes are unchanged by a step without solver
+        d.fe1[scur + gi] = d.fe1[sprev + gi];
+        d.fn1[scur + gi] = d.fn1[sprev + gi];
+      }
       courant_cell(d, h1, d.qx[gi], d.qy[gi], dtc, hm);
     }
     reduce_courant(d, S, dtc, hm);
@@ -481,7 +491,7 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
       qy = d.qy[gi];
       if (r >= 1 && r <= d.nr && q >= 1 && q <= d.nc) {
         cl = C_INT;
-        if (d.flags[gi] & FX_F_WALL) cl |= C_WALL;
+        if (d.flags[sprev + gi] & FX_F_WALL) cl |= C_WALL;
         if (melt_on && zb != d.nodata) z = z + melt_depth(d, c, gi);
         const double h1 = fmax(0.0, z - zb);
         if (h1 <= d.hdry) {
@@ -542,10 +552,10 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
       const int k = S.stale_list[i];
       const int fr = k % FXN, fc = k / FXN;
       const long long gi = fx_ix(d, irow0 - 1 + fr, icol0 - 1 + fc);
-      S.f[0][k] = d.fe1[gi];
+      S.f[0][k] = d.fe1[sprev + gi];
       S.f[1][k] = d.fe2[gi];
       S.f[2][k] = d.fe3[gi];
-      S.f[3][k] = d.fn1[gi];
+      S.f[3][k] = d.fn1[sprev + gi];
       S.f[4][k] = d.fn2[gi];
       S.f[5][k] = d.fn3[gi];
     }
@@ -560,24 +570,18 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
     const int fP = (ly + 1) * FXN + (lx + 1), fW = (ly + 1) * FXN + lx, fS = ly * FXN + (lx + 1);
     const unsigned char cl = S.cls[sP];
     const bool wall = cl & C_WALL;
-    const uint8_t fl = d.flags[gi];
+    const uint8_t fl = d.flags[sprev + gi];
     const double zb = S.zb[sP];
     const double z1 = S.z[sP];
     const double zpre = d.z[gi];
-    const double dxy = d.dxy;
 
-    // add_meteo side effects on this cell (common.cpp:214-234)
+    // add_meteo's h0 (common.cpp:223): the depth after the melt, or the
+    // Courant scan's copy of h (main.cpp:305) for cells it skips. Its solute
+    // dilution (:226-234) is applied by the ADE sweep (fx_ade.cu).
     double h0v = fmax(0.0, zpre - zb);
     if (melt_on && zb != d.nodata) {
-      const double hp = fmax(zpre - zb, 0.0);
       h0v = fmax(z1 - zb, 0.0);
-      if (d.ade && hp != 0.0) {
-        const double mi = melt_depth(d, c, gi);
-        for (int k = 0; k < d.nchem; ++k) {
-          double* cp = d.conc + k * d.plane + gi;
-          *cp = (*cp * hp + (mi * c.mconc)) / (h0v);
-        }
-      }
+      if (d.ade) d.hpm[scur + gi] = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
     }
     // Loop 1 wet time (:69-70)
     if (!(cl & C_DRY)) d.twet[gi] += dtl / 3600;
@@ -585,9 +589,9 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
     // Loop 3 (:93-120)
     double dh = 0.0, dqx = 0.0, dqy = 0.0, qxfP = 0.0, qyfP = 0.0;
     if (!wall) {
-      dh = ((S.f[0][fW] - S.f[0][fP]) / dxy + (S.f[3][fS] - S.f[3][fP]) / dxy) * dtl;
-      dqx = ((S.f[1][fW] - S.f[1][fP]) / dxy + (S.f[4][fS] - S.f[4][fP]) / dxy) * dtl;
-      dqy = ((S.f[2][fW] - S.f[2][fP]) / dxy + (S.f[5][fS] - S.f[5][fP]) / dxy) * dtl;
+      dh = (fx_div_dxy(d, S.f[0][fW] - S.f[0][fP]) + fx_div_dxy(d, S.f[3][fS] - S.f[3][fP])) * dtl;
+      dqx = (fx_div_dxy(d, S.f[1][fW] - S.f[1][fP]) + fx_div_dxy(d, S.f[4][fS] - S.f[4][fP])) * dtl;
+      dqy = (fx_div_dxy(d, S.f[2][fW] - S.f[2][fP]) + fx_div_dxy(d, S.f[5][fS] - S.f[5][fP])) * dtl;
       qxfP = S.f[0][fP] * dtl;
       qyfP = S.f[3][fP] * dtl;
     }
@@ -623,11 +627,11 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
       }
     }
     d.z[gi] = z;
-    d.h[gi] = h;
+    d.h[scur + gi] = h;
     d.qx[gi] = qx;
     d.qy[gi] = qy;
-    d.h0[gi] = h0v;
-    d.flags[gi] = (fl & FX_F_WALL) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+    d.h0[scur + gi] = h0v;
+    d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
     // Fluxes computed this step become the grid values (stale ones are
     // already there). fe_2/fe_3/fn_2/fn_3 are read back only when this cell
     // is dry with four dry neighbours at a later solver step; a cell that
@@ -639,16 +643,19 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
       const bool computed =
           !(clP & C_DRY) || !((S.cls[sidx(lx + 1, ly + 2)] & C_DRY) && (S.cls[sidx(lx + 3, ly + 2)] & C_DRY) &&
                               (S.cls[sidx(lx + 2, ly + 1)] & C_DRY) && (S.cls[sidx(lx + 2, ly + 3)] & C_DRY));
-      if (computed) {
-        d.fe1[gi] = S.f[0][fP];
-        d.fn1[gi] = S.f[3][fP];
-        if (d.store_all_fluxes || !(h > d.hdry)) {
-          d.fe2[gi] = S.f[1][fP];
-          d.fe3[gi] = S.f[2][fP];
-          d.fn2[gi] = S.f[4][fP];
-          d.fn3[gi] = S.f[5][fP];
-        }
+      // fe_1/fn_1 of every cell go to this step's slot: computed ones, or the
+      // stale ones carried over (already in S.f for stale cells).
+      d.fe1[scur + gi] = S.f[0][fP];
+      d.fn1[scur + gi] = S.f[3][fP];
+      if (computed && (d.store_all_fluxes || !(h > d.hdry))) {
+        d.fe2[gi] = S.f[1][fP];
+        d.fe3[gi] = S.f[2][fP];
+        d.fn2[gi] = S.f[4][fP];
+        d.fn3[gi] = S.f[5][fP];
       }
+    } else if (scur != sprev) {
+      d.fe1[scur + gi] = 0.0;  // walls: never written in the reference
+      d.fn1[scur + gi] = 0.0;
     }
     courant_cell(d, h, qx, qy, dtc, hm);
   }
@@ -657,13 +664,13 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
 
 // Courant scan of the state as uploaded (the scan at the top of the first
 // step). Also used after a host edit of the state.
-__global__ void k_courant_scan(fx_dev d) {
-  const int irow = 1 + blockIdx.x * TX + threadIdx.x, icol = 1 + blockIdx.y * TY + threadIdx.y;
+__global__ void __launch_bounds__(NTHREADS) k_courant_scan(fx_dev d) {
+  const int irow = 1 + blockIdx.x * BX + threadIdx.x, icol = 1 + blockIdx.y * BY + threadIdx.y;
   __shared__ HydroSmem S;
   double dtc = __longlong_as_double(0x7ff0000000000000LL), hm = 0.0;
   if (irow <= d.nr && icol <= d.nc) {
     const long long gi = fx_ix(d, irow, icol);
-    courant_cell(d, d.h[gi], d.qx[gi], d.qy[gi], dtc, hm);
+    courant_cell(d, d.h[fx_slot(d, d.ctl->steps) + gi], d.qx[gi], d.qy[gi], dtc, hm);
   }
   reduce_courant(d, S, dtc, hm);
 }
@@ -711,22 +718,51 @@ __global__ void k_finalize(fx_dev d) {
   if (c.active) c.it = c.it + 1;
   c.print_pending = c.tim >= c.print_next;
   c.steps = c.steps + 1;
+  fx_steprec& r = c.rec[c.steps % d.nslot];
+  r.dtfl = c.dtfl;
+  r.meteoi = c.meteoi;
+  r.meteo_rate = c.meteo_rate;
+  r.mconc = c.mconc;
+  r.step = c.steps;
+  r.batch = c.batch;
+  r.live = 1;
+  r.active = c.active;
+  r.it = c.it;
   c.acc_dtmin = (unsigned long long)__double_as_longlong(__longlong_as_double(0x7ff0000000000000LL));
   c.acc_hmax = 0ull;
   c.live = 1;
+}
+
+// Opens a batch of steps whose ADE sweeps run together (fx_ade.cu).
+__global__ void k_batch_begin(fx_dev d) { d.ctl->batch = d.ctl->batch + 1; }
+
+// Sets the bed flags that never change (NODATA bed) in every slot plane.
+__global__ void k_mark_static(fx_dev d) {
+  const long long n = d.plane;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int icol = (int)(i / d.ld), irow = (int)(i % d.ld) - FX_ROFF;
+    if (irow < 1 || irow > d.nr || icol < 1 || icol > d.nc) continue;
+    const bool nod = d.zb[i] == d.nodata;
+    for (int k = 0; k < d.nslot; ++k) {
+      uint8_t& f = d.flags[k * d.plane + i];
+      f = (uint8_t)((f & ~FX_F_NODATA) | (nod ? FX_F_NODATA : 0));
+    }
+  }
 }
 
 }  // namespace fx
 
 // Launch helpers used by fx_capi.cu.
 void fx_launch_finalize(const fx_dev& d, cudaStream_t s) { fx::k_finalize<<<1, 1, 0, s>>>(d); }
+void fx_launch_batch_begin(const fx_dev& d, cudaStream_t s) { fx::k_batch_begin<<<1, 1, 0, s>>>(d); }
+void fx_launch_mark_static(const fx_dev& d, cudaStream_t s) { fx::k_mark_static<<<592, 256, 0, s>>>(d); }
 
 void fx_launch_hydro(const fx_dev& d, cudaStream_t s) {
-  dim3 b(fx::TX, fx::TY), g((d.nr + fx::TX - 1) / fx::TX, (d.nc + fx::TY - 1) / fx::TY);
+  dim3 b(fx::BX, fx::BY), g((d.nr + fx::TX - 1) / fx::TX, (d.nc + fx::TY - 1) / fx::TY);
   fx::k_hydro<<<g, b, 0, s>>>(d);
 }
 
 void fx_launch_courant_scan(const fx_dev& d, cudaStream_t s) {
-  dim3 b(fx::TX, fx::TY), g((d.nr + fx::TX - 1) / fx::TX, (d.nc + fx::TY - 1) / fx::TY);
+  dim3 b(fx::BX, fx::BY), g((d.nr + fx::BX - 1) / fx::BX, (d.nc + fx::BY - 1) / fx::BY);
   fx::k_courant_scan<<<g, b, 0, s>>>(d);
 }

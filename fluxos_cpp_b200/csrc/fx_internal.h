@@ -21,6 +21,7 @@ struct fx_ctx {
   long long bytes = 0;
   int ade_strips = 0;
   int ade_blocks = 0;
+  int batch_steps = 1;         // steps per batch (ADE sweeps in flight)
   bool prepared = false;
   bool graph_dirty = true;
   bool store_all_opt = false;

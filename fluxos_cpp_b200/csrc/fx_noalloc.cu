@@ -47,8 +47,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[FX_NOALLOC_SCRA
 namespace {
 
 constexpr int kMaxDevices = 64;
-constexpr size_t kCtlBytes = 256;  // fx_ctl, rounded up
-static_assert(sizeof(fx_ctl) <= kCtlBytes, "control block does not fit its slot");
+constexpr size_t kCtlBytes = (sizeof(fx_ctl) + 255) & ~(size_t)255;  // fx_ctl, rounded up
 
 struct DeviceSetup {
   bool ready = false;
@@ -68,6 +67,13 @@ __global__ void k_noalloc_ctl(fx_ctl* ctl, double dtfl) {
   c.it = 2;
   c.steps = 1;
   c.stop_after = 1;
+  c.batch = 1;
+  c.rec[0].dtfl = dtfl;
+  c.rec[0].step = 1;
+  c.rec[0].batch = 1;
+  c.rec[0].live = 1;
+  c.rec[0].active = 1;
+  c.rec[0].it = 2;
   *ctl = c;
 }
 
@@ -85,7 +91,7 @@ extern "C" int fx_adesolver_noalloc(double* conc, const double* h, const double*
   if (ld < nrows + 2 + FX_ROFF || (((long long)ld * (ncols + 2)) & 3) != 0)
     return fx_fail(nullptr, FX_ERR_ARG,
                    "fx_adesolver_noalloc: ld must be >= nrows + 3 and ld * (ncols + 2) a multiple of 4");
-  if (((size_t)flags & 3) != 0 || ((size_t)conc & 7) != 0 || ((size_t)h & 7) != 0 || ((size_t)h0 & 7) != 0 ||
+  if (((size_t)flags & 3) != 0 || ((size_t)conc & 15) != 0 || ((size_t)h & 7) != 0 || ((size_t)h0 & 7) != 0 ||
       ((size_t)fe_1 & 7) != 0 || ((size_t)fn_1 & 7) != 0)
     return fx_fail(nullptr, FX_ERR_ARG, "fx_adesolver_noalloc: misaligned array");
   if (!(dtfl > 0.0)) return fx_fail(nullptr, FX_ERR_ARG, "fx_adesolver_noalloc: dtfl must be > 0");
@@ -131,10 +137,9 @@ extern "C" int fx_adesolver_noalloc(double* conc, const double* h, const double*
   d.nc = ncols;
   d.ld = ld;
   d.nchem = 1;
+  d.nslot = 1;
   d.plane = (long long)ld * (ncols + 2);
-  d.dxy_u = (unsigned)dxy;
-  d.dxy = (double)dxy;
-  d.arbase = (double)((unsigned long)dxy * (unsigned long)dxy);
+  fx_set_cell_size(d, dxy);
   d.ade = 1;
   d.dcoef[0] = d_coef;
   d.conc = conc;

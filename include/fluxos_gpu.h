@@ -63,6 +63,7 @@ typedef struct fx_params {
   int ade;           /* EXTERNAL_MODULES.ADE_TRANSPORT.STATUS */
   int volrat_mode;   /* domain-edge weir: 0 = weir formula (default), 1 = closed */
   double d_coef[FX_MAX_CHEM]; /* dispersion coefficient per solute */
+  int steps_in_flight; /* steps whose ADE sweeps run in one launch, 1..15 (0 = 8) */
 } fx_params;
 
 /* Clock and status read back from the device. */
@@ -131,7 +132,8 @@ int fx_time_steps(fx_ctx* ctx, int nsteps, double* ms_total, double* ms_hydro, d
  * inside a fixed memory budget): one ADE step, ADEsolver_calc for one solute
  * with it > 1, applied in place to `conc` on device arrays the caller owns.
  * Arrays hold (nrows+2) x (ncols+2) cells; cell (irow, icol) is element
- * icol*ld + irow + 1 (ld >= nrows+3, ld*(ncols+2) a multiple of 4); `flags`
+ * icol*ld + irow + 1 (ld >= nrows+3, ld*(ncols+2) a multiple of 4; conc
+ * 16-byte aligned, the other grids 8-byte, flags 4-byte); `flags`
  * holds one byte per cell: bit 0 ldry, bit 1 ldry_prev, bit 2 wall. h, h0,
  * fe_1, fn_1 are the depth after and before the hydrodynamic update and the
  * face fluxes of that update; dtfl is its time step. The call allocates

@@ -8,13 +8,14 @@ import pyoracle as P
 STATE = ("z", "h", "qx", "qy", "twet", "h0", "fe_1", "fe_2", "fe_3", "fn_1", "fn_2", "fn_3")
 
 
-def domain_from_oracle(ora, sc, volrat_mode=0, store_all=True):
+def domain_from_oracle(ora, sc, volrat_mode=0, store_all=True, steps_in_flight=0):
     nchem = sc.nchem
     d = fx.Domain(sc.nrows, sc.ncols, sc.dxy, nchem=nchem, nodata=float(sc.nodata),
                   hdry=ora.scalar("hdry"), ntim=ora.scalar("ntim"), print_step=sc.print_step,
                   print_next=ora.scalar("print_next"), tim=ora.scalar("tim"), ade=sc.ade,
                   volrat_mode=volrat_mode,
-                  d_coef=list(sc.d_coefs) if sc.d_coefs else [sc.d_coef])
+                  d_coef=list(sc.d_coefs) if sc.d_coefs else [sc.d_coef],
+                  steps_in_flight=steps_in_flight)
     for k in ("zb",) + STATE:
         d.upload(k, ora.grid(k))
     for k in range(nchem):

@@ -97,16 +97,19 @@ def test_flux_store_skipping_changes_nothing(tmp_path):
     assert np.array_equal(a.download_flags()["ldry"], b.download_flags()["ldry"])
 
 
-def test_dry_start_melt_transition(tmp_path):
+@pytest.mark.parametrize("in_flight", [1, 3, 8])
+def test_dry_start_melt_transition(in_flight, tmp_path):
     """Initially dry domain: Courant-only steps of a whole print interval,
     melt until the dry threshold is passed, then the solver switches on
-    (the add_meteo ldry quirk and the it == 1 ADE skip are on this path)."""
+    (the add_meteo ldry quirk and the it == 1 ADE skip are on this path).
+    Outputs fall inside batches of ADE steps in flight, for several batch
+    sizes."""
     sc = S.plane_scenario(48, 40, seed=3)
     sc.meteo = ((0.0, 80.0, 1.0), (3000.0, 80.0, 1.0))
     sc.horizon = 3000.0
     sc.write(str(tmp_path))
     ora = P.OracleRun(str(tmp_path), sc, 0)
-    d = GP.domain_from_oracle(ora, sc, 0)
+    d = GP.domain_from_oracle(ora, sc, 0, steps_in_flight=in_flight)
     for n in (1, 2, 3, 50, 400, 2000):
         GP.advance_oracle(ora, n)
         GP.advance_domain(d, n)
