@@ -145,10 +145,11 @@ def full(sc, interior: np.ndarray, fill: float = 0.0) -> np.ndarray:
     return g
 
 
-def build_domain(sc, h, conc):
+def build_domain(sc, h, conc, in_flight: int = 8):
     import fluxos_cpp_b200 as fx
     d = fx.Domain(sc.nrows, sc.ncols, sc.dxy, nchem=1, hdry=sc.ks, ntim=sc.horizon,
-                  print_step=sc.print_step, print_next=sc.print_step, ade=True, d_coef=[sc.d_coef])
+                  print_step=sc.print_step, print_next=sc.print_step, ade=True, d_coef=[sc.d_coef],
+                  steps_in_flight=in_flight)
     zb_raw = full(sc, sc.dem.astype(np.float64))
     d.initiate(zb_raw)
     d.set_forcing(forcing_table(sc))
@@ -245,9 +246,9 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import fluxos_cpp_b200 as fx
     n = args.size
-    k_batch = 8  # steps per ADE launch (fx_params.steps_in_flight default)
+    k_batch = args.in_flight  # steps per ADE launch
     sc, h, conc = make_workload(n)
-    d = build_domain(sc, h, conc)
+    d = build_domain(sc, h, conc, k_batch)
     cells = n * n
     d.step(args.warmup)
     if world > 1:
@@ -353,6 +354,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-crop", type=int, default=2048)
     ap.add_argument("--cpu-steps", type=int, default=12)
+    ap.add_argument("--in-flight", type=int, default=8, help="steps per ADE launch (1..15)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

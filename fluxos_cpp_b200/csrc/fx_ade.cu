@@ -280,23 +280,42 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, double D, double dt, b
   qfn_out = qfn;
 }
 
-// Wait until a progress counter reaches `need` warp steps of step `tag`;
-// false if the wait gave up (the error flag is then set). A null counter is
-// no dependency.
-__device__ __forceinline__ bool wait_progress(const fx_dev& d, const unsigned long long* prog,
-                                              unsigned long long tag, int need) {
-  if (!prog) return true;
-  const unsigned long long want = (tag << 32) | (unsigned)need;
+// The three progress counters a unit depends on: the west strip of its step
+// and, on the previous step of the batch, its own strip and the next one.
+// The last values seen are kept, so a requirement the producer has already
+// passed costs no memory access; otherwise all three are reloaded together
+// (one round trip). A null counter is no dependency.
+struct Deps {
+  const unsigned long long *w, *p0, *p1;
+  unsigned long long tag_w, tag_p;
+  unsigned long long seen_w, seen_p0, seen_p1;
+};
+
+__device__ __forceinline__ bool dep_ok(const unsigned long long* p, unsigned long long seen,
+                                       unsigned long long tag, int need) {
+  return !p || seen >= ((tag << 32) | (unsigned)need);
+}
+
+// Wait until the counters reach the given warp-step counts; false if the wait
+// gave up (the error flag is then set).
+__device__ __forceinline__ bool wait_deps(const fx_dev& d, Deps& D, int need_w, int need_p0, int need_p1) {
   long long it = 0;
   for (;;) {
-    const unsigned long long v = ld_acquire(prog);
-    if (__all_sync(0xffffffffu, v >= want)) return true;
+    const bool ok = dep_ok(D.w, D.seen_w, D.tag_w, need_w) && dep_ok(D.p0, D.seen_p0, D.tag_p, need_p0) &&
+                    dep_ok(D.p1, D.seen_p1, D.tag_p, need_p1);
+    if (__all_sync(0xffffffffu, ok)) return true;
     const bool stop = (++it > SPIN_LIMIT) || (*(volatile int*)&d.ctl->error != 0);
     if (__any_sync(0xffffffffu, stop)) {
       if ((threadIdx.x & 31) == 0) atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
       return false;
     }
-    __nanosleep(64);
+    if (it > 1) __nanosleep(it < 8 ? 64 : (it < 64 ? 256 : 1024));
+    const unsigned long long a = D.w ? ld_acquire(D.w) : 0ull;
+    const unsigned long long b = D.p0 ? ld_acquire(D.p0) : 0ull;
+    const unsigned long long c = D.p1 ? ld_acquire(D.p1) : 0ull;
+    D.seen_w = a;
+    D.seen_p0 = b;
+    D.seen_p1 = c;
   }
 }
 
@@ -366,14 +385,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
     const double* bnd_in = d.ade_bnd + unit_index(slot, k, s) * bnd_stride;
     double* bnd_out = (s + 1 < nstrips) ? d.ade_bnd + unit_index(slot, k, s + 1) * bnd_stride : nullptr;
     bool bail = false;
-
+    Deps dep;
+    dep.w = prog_w;
+    dep.p0 = prog_p0;
+    dep.p1 = prog_p1;
+    dep.tag_w = tag;
+    dep.tag_p = tag - 1;
+    dep.seen_w = dep.seen_p0 = dep.seen_p1 = 0ull;
     // the previous step must have written every column prefetched before a
-    // check: lanes 0..29 of its strip s, lanes 0..1 of its strip s + 1
-    auto prev_ready = [&](int col) {
-      return wait_progress(d, prog_p0, tag - 1, min(col + ROWS, T)) &&
-             wait_progress(d, prog_p1, tag - 1, min(col + 2, T));
-    };
-    if (!prev_ready(DIST + 3)) bail = true;
+    // check (lanes 0..29 of its strip s, lanes 0..1 of its strip s + 1), and
+    // the west strip of this step the boundary columns read in the chunk
+    auto need_p0 = [&](int col) { return min(col + ROWS, T); };
+    auto need_p1 = [&](int col) { return min(col + 2, T); };
+    if (!wait_deps(d, dep, min(CHUNK - 1 + ROWS, T), need_p0(DIST + 3), need_p1(DIST + 3))) bail = true;
 
     // prime the ring: columns iy0 .. iy0 + DIST + 2 of this lane's row
     const int iy0 = 1 - lane;
@@ -397,17 +421,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
     double bw_c = 0.0, bw_pfe = 0.0, bw_b = 0.0, bn_c = 0.0, bn_pfe = 0.0, bn_b = 0.0;
     int bw_ld = 0, bn_ld = 0;
     if (!bail && prog_w) {
-      if (!wait_progress(d, prog_w, tag, min(CHUNK - 1 + ROWS, T))) {
-        bail = true;
-      } else {
-        const int iyb = 1 + lane;
-        if (lane < CHUNK && iyb <= d.nc) {
-          const double* p = bnd_in + (long long)iyb * 3;
-          bn_c = __ldcg(p);
-          bn_pfe = __ldcg(p + 1);
-          bn_b = __ldcg(p + 2);
-          bn_ld = d.flags[S.cur + fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
-        }
+      const int iyb = 1 + lane;
+      if (lane < CHUNK && iyb <= d.nc) {
+        const double* p = bnd_in + (long long)iyb * 3;
+        bn_c = __ldcg(p);
+        bn_pfe = __ldcg(p + 1);
+        bn_b = __ldcg(p + 2);
+        bn_ld = d.flags[S.cur + fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
       }
     }
 
@@ -417,17 +437,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
         bw_pfe = bn_pfe;
         bw_b = bn_b;
         bw_ld = bn_ld;
-        // columns lane 0 prefetches during this chunk
-        if (!prev_ready(tau + CHUNK + DIST + 3)) {
+        // columns lane 0 prefetches during this chunk, and the next chunk's
+        // boundary (loaded now, used in CHUNK steps)
+        const int col = tau + CHUNK + DIST + 3;
+        if (!wait_deps(d, dep, min(tau + 2 * CHUNK - 1 + ROWS, T), need_p0(col), need_p1(col))) {
           bail = true;
           break;
         }
         if (prog_w && tau + CHUNK < T) {
-          // the next chunk's boundary: wait for it now, use it in CHUNK steps
-          if (!wait_progress(d, prog_w, tag, min(tau + 2 * CHUNK - 1 + ROWS, T))) {
-            bail = true;
-            break;
-          }
           const int iyb = tau + CHUNK + 1 + lane;
           bn_c = bn_pfe = bn_b = 0.0;
           bn_ld = 0;
