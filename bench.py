@@ -1,18 +1,30 @@
 #!/usr/bin/env python
 """Benchmark of the FLUXOS-OVERLAND explicit step on one B200 per rank.
 
-Workload (the large single-domain configuration): 4096 x 4096 cells of 2 m,
-spectral-fractal terrain (P(k) ~ k^-3, seed 1, 0-3 m relief) with 200
-circular depressions, a smooth melt-rate field of 5-40 mm/day (seed 2) as a
-per-cell multiplier of the forcing rate, Manning n ~ U[0.03, 0.15], one
-solute (D = 0.01 m^2/s). All inputs are seeded synthetic stand-ins generated
-by fluxos_cpp_b200.scenarios. The state starts wet (a 5 mm film plus water
-ponded in the depressions), as a snapshot taken during melt would be.
+Headline workload (the large single-domain configuration, FP64 plain vs
+FP32): 4096 x 4096 cells of 2 m, spectral-fractal terrain (P(k) ~ k^-3,
+seed 1, 0-3 m relief) with 200 circular depressions, a smooth melt-rate
+field of 5-40 mm/day (seed 2) as a per-cell multiplier of the forcing rate,
+Manning n ~ U[0.03, 0.15], one solute (D = 0.01 m^2/s). All inputs are seeded
+synthetic stand-ins generated by fluxos_cpp_b200.scenarios. The state starts
+wet (a 5 mm film plus water ponded in the depressions), as a snapshot taken
+during melt would be.
 
 A step is one iteration of the reference's loop (main.cpp:271-406): Courant
 dt, melt forcing, the hydrodynamic update and the ADE sweep over all cells.
-metric = cell-updates/s = cells x steps / device time; with N ranks each rank
-runs its own replica and value is the sum (weak scaling, no collective).
+metric = cell-updates/s = cells x steps / device time. `value` is the FP32
+state's rate; the FP64 path (the reference's arithmetic) runs the same steps
+from the same start, and the FP32 depth/discharge error and both runs'
+mass-balance error are measured on the states after those steps. With N
+ranks each rank runs its own replica and value is the sum (weak scaling, no
+collective).
+
+Also reported on the same line (skipped with --no-mix / --no-serve):
+* mix: the 64-scenario ensemble (sizes 256^2-2048^2) advanced as one FP32
+  batch (autotuned tiles), against the same scenarios as an FP64 batch and
+  run one by one on the plain FP64 path;
+* serve: a bounded sample of the serving configuration's request stream
+  through the continuous-batching loop, with p50/p99 latency.
 
 --impl reference times the FLUXOS reference sources compiled in oracle/_ref
 (OpenMP hydrodynamics, serial ADE) on the host cores instead.
@@ -34,15 +46,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s FP32 vs FP64 at stated depth/mass error; p50/p99 request latency"
-# Algorithmic bytes per cell-update of the step (read + write of h, qx, qy and
-# the solute, read of bed and wall, read of Manning n and the melt field):
-# 2*8*(3+1) + 8 + 1 + 8 + 4 = 85 B, and 89 B when the melt field is 8 bytes
-# as here (FP64 storage). Split by kernel: the hydrodynamic kernel moves the
-# flow state, bed, wall, n and melt (2*8*3 + 8 + 1 + 8 + 8 = 73 B), the ADE
-# sweep the solute (2*8 = 16 B).
-ALG_BYTES_STEP = 89
-ALG_BYTES_HYDRO = 73
-ALG_BYTES_ADE = 16
+# Algorithmic bytes per cell-update, per kernel (read + write of the flow
+# state, read of the bed, wall flag, Manning n and melt field; read + write of
+# the solute):
+#   FP64: hydro 2*8*3 (h or z, qx, qy) + 8 (zb) + 1 + 8 (n) + 8 (melt) = 73 B,
+#         ADE 2*8 = 16 B, step 89 B;
+#   FP32: hydro 2*4*3 (eta, qx, qy) + 8 (bed differences sx, sy) + 1 + 4 + 4
+#         = 41 B, ADE 2*4 = 8 B, step 49 B.
+ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
+             "fp32": {"k_hydro": 41, "k_ade_sweep": 8, "step": 49}}
 
 
 def _rank():
@@ -121,54 +133,23 @@ def gpu_id_of_device0() -> str:
 
 
 def make_workload(n: int, seed: int = 1):
-    """Terrain, melt multiplier, Manning n, forcing table and the wet start."""
+    """The large-domain scenario with a wet start: a 5 mm film plus water
+    ponded in the depressions, solute 1 where the depth exceeds 10 mm."""
     from fluxos_cpp_b200 import scenarios as S
     sc = S.fractal_scenario(n, dxy=2, seed=seed, melt_seed=seed + 1, extensions=True)
     dem = sc.dem.astype(np.float64)
     film = 0.005
     h = film + np.maximum(S.box3(S.box3(dem)) - dem, 0.0)
-    conc = np.where(h > 2 * film, 1.0, 0.0)
-    return sc, h, conc
+    sc.init_h = h
+    sc.init_qx = np.zeros_like(h)
+    sc.init_qy = np.zeros_like(h)
+    sc.init_conc = [np.where(h > 2 * film, 1.0, 0.0)]
+    return sc
 
 
-def forcing_table(sc) -> np.ndarray:
-    tab = np.zeros((3, 2000), dtype=np.float32)
-    rows = list(sc.meteo) + [(1.0e9, 0.0, 0.0), (sc.horizon, 0.0, 0.0)]
-    for a, (t, r, c) in enumerate(rows, start=1):
-        tab[:, a] = (t, r, c)
-    return tab
-
-
-def full(sc, interior: np.ndarray, fill: float = 0.0) -> np.ndarray:
-    g = np.full((sc.ncols + 2, sc.nrows + 2), fill)
-    g[1:-1, 1:-1] = interior.T
-    return g
-
-
-def build_domain(sc, h, conc, in_flight: int = 8):
-    import fluxos_cpp_b200 as fx
-    d = fx.Domain(sc.nrows, sc.ncols, sc.dxy, nchem=1, hdry=sc.ks, ntim=sc.horizon,
-                  print_step=sc.print_step, print_next=sc.print_step, ade=True, d_coef=[sc.d_coef],
-                  steps_in_flight=in_flight)
-    zb_raw = full(sc, sc.dem.astype(np.float64))
-    d.initiate(zb_raw)
-    d.set_forcing(forcing_table(sc))
-    d.set_melt_field(full(sc, sc.melt_mult, 1.0))
-    d.set_manning(full(sc, sc.manning, 0.0))
-    zb = d.download("zb")
-    z = zb.copy()
-    z[1:-1, 1:-1] += h.T
-    hh = np.zeros_like(zb)
-    hh[1:-1, 1:-1] = h.T
-    d.upload("z", z)
-    d.upload("h", hh)
-    d.upload("conc", full(sc, conc))
-    fl = d.download_flags()
-    ld = np.zeros_like(fl["ldry"])
-    ld[1:-1, 1:-1] = np.where(h.T > sc.ks, 0.0, 1.0)
-    d.upload_flags(ld, fl["wall"])
-    d.prepare()
-    return d
+def build_domain(sc, in_flight: int = 8, precision: str = "fp64"):
+    from fluxos_cpp_b200 import scenarios as S
+    return S.make_domain(sc, precision=precision, steps_in_flight=in_flight)
 
 
 def e2e_run(d, sc, steps: int):
@@ -236,6 +217,129 @@ def cpu_reference_run(sc, h, conc, warmup: int, steps: int, crop: int):
                       f"serial ADE"}
 
 
+def measure_domain(d, steps: int, warmup: int, cells: int, precision: str, peak: float, gpu: str):
+    """Warm-up, then `steps` timed steps (CUDA events on the domain's stream
+    around every launch, fx_time_steps); roofline of the dominant kernel."""
+    d.step(warmup)
+    sampler = ClockSampler(gpu)
+    sampler.start()
+    ms_total, ms_hydro, ms_ade = d.time_steps(steps)
+    clocks = sampler.stop()
+    st = d.status()
+    if st["device_error"]:
+        raise RuntimeError("device error during the timed steps")
+    alg = ALG_BYTES[precision]
+    ms_h, ms_a = ms_hydro / steps, ms_ade / steps
+    kern = {"k_hydro": ms_h, "k_ade_sweep": ms_a}
+    dom = max(kern, key=kern.get)
+    achieved = cells * alg[dom] / (kern[dom] / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(f"{dom}_{precision}")
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": traffic, "alg_bytes_per_cell": alg[dom],
+            "ms_per_step": {"k_hydro": round(ms_h, 4), "k_ade_sweep": round(ms_a, 4)},
+            "step_alg_GBps": round(cells * alg["step"] / (ms_total / steps / 1e3) / 1e9, 1)}
+    return {"ms_total": ms_total, "value": cells * steps / (ms_total / 1e3), "roofline": roof,
+            "clocks": clocks}
+
+
+def accuracy_of(d32, d64, w32: float, w64: float, hdry: float) -> dict:
+    from fluxos_cpp_b200 import accuracy as A
+    e = A.state_errors(d32, d64, hdry)
+    b32, b64 = A.water_balance(d32, w32), A.water_balance(d64, w64)
+    return {"against": "FP64 path (itself within 1e-10 per cell of the reference, tests/test_gpu_parity.py)",
+            "steps": int(d32.status()["steps"]),
+            "depth_l1_rel": e["depth"]["l1_rel"], "depth_linf_m": e["depth"]["linf_abs"],
+            "depth_linf_rel": e["depth"]["linf_rel"],
+            "discharge_l1_rel": e["discharge"]["l1_rel"], "discharge_linf_m2s": e["discharge"]["linf_abs"],
+            "solute_l1_rel": e["solute_mass_density"][0]["l1_rel"],
+            "wet_cells_differ": e["wet_cells"]["differ"], "wet_cells": e["wet_cells"]["ref"],
+            "mass_balance_rel_fp32": b32["rel_err"], "mass_balance_rel_fp64": b64["rel_err"]}
+
+
+def run_mix(args, peak: float) -> dict:
+    """The 64-scenario ensemble: FP32 batch vs FP64 batch vs FP64 one by one."""
+    import torch
+    import fluxos_cpp_b200 as fx
+    from fluxos_cpp_b200 import scenarios as S
+    from concurrent.futures import ThreadPoolExecutor
+    t0 = time.perf_counter()
+    scs = S.ensemble_scenarios(args.mix_count, seed=3)
+    gen_s = time.perf_counter() - t0
+    cells = [sc.nrows * sc.ncols for sc in scs]
+    steps = args.mix_steps
+
+    def batch_rate(precision):
+        doms = [S.make_domain(sc, precision=precision, steps_in_flight=8) for sc in scs]
+        b = fx.Batch()
+        for d in doms:
+            b.add(d)
+        tuned = b.autotune(4) if precision == "fp32" else (8, 8)
+        b.step(args.warmup)
+        s0 = [d.status()["steps"] for d in doms]
+        stream = torch.cuda.ExternalStream(b.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        done = sum((d.status()["steps"] - a) * c for d, a, c in zip(doms, s0, cells))
+        nbytes = sum(d.device_bytes() for d in doms)
+        b.close()
+        for d in doms:
+            d.close()
+        return done / (ms / 1e3), ms, tuned, nbytes
+
+    r32, ms32, tuned, bytes32 = batch_rate("fp32")
+    r64b, ms64b, _, bytes64 = batch_rate("fp64")
+    # plain FP64 path: each scenario alone, one after another
+    tot_ms, tot_cells = 0.0, 0
+    for sc, c in zip(scs, cells):
+        d = S.make_domain(sc, precision="fp64", steps_in_flight=8)
+        d.step(args.warmup)
+        s0 = d.status()["steps"]
+        ms, _, _ = d.time_steps(steps)
+        tot_ms += ms
+        tot_cells += (d.status()["steps"] - s0) * c
+        d.close()
+    r64 = tot_cells / (tot_ms / 1e3)
+    return {"scenarios": len(scs), "cells": int(sum(cells)), "sizes": f"{min(sc.nrows for sc in scs)}^2.."
+            f"{max(sc.nrows for sc in scs)}^2 (log-uniform, seed 3)", "steps": steps,
+            "fp32_batch_cell_updates_per_s": r32, "fp32_batch_ms": round(ms32, 3),
+            "fp32_batch_alg_GBps": round(r32 * ALG_BYTES["fp32"]["step"] / 1e9, 1),
+            "fp32_batch_hbm_frac": round(r32 * ALG_BYTES["fp32"]["step"] / 1e9 / peak, 4),
+            "fp64_batch_cell_updates_per_s": r64b, "fp64_plain_cell_updates_per_s": r64,
+            "fp32_batch_over_fp64_plain": round(r32 / r64, 3),
+            "fp32_batch_over_fp64_batch": round(r32 / r64b, 3),
+            "autotuned": {"tile_rows": tuned[0], "steps_in_flight": tuned[1]},
+            "device_bytes_fp32": bytes32, "device_bytes_fp64": bytes64,
+            "host_generation_s": round(gen_s, 1),
+            "note": "per-scenario dt; timed region = one fx_batch_step of all members (CUDA events on "
+                    "the batch stream); plain FP64 = each scenario alone through fx_time_steps"}
+
+
+def run_serve(args) -> dict:
+    from fluxos_cpp_b200 import serve
+    reqs = serve.poisson_requests(rate=4.0, duration=args.serve_seconds, seed=4,
+                                  horizon_scale=args.serve_horizon_scale)
+    srv = serve.Server(cap_bytes=150e9, chunk_steps=32)
+    stats = srv.run(reqs)
+    srv.close()
+    stats.update({"arrivals": f"Poisson 4/s for {args.serve_seconds:g} s (seed 4)",
+                  "grids": "128^2..4096^2 log-uniform", "solutes": "1-3",
+                  "horizon": f"1-12 h x {args.serve_horizon_scale:g} (bounded sample)",
+                  "admission_cap_bytes": 150e9, "precision": "fp32",
+                  "latency": "arrival to retirement, including host-side input generation"})
+    return stats
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -244,77 +348,75 @@ def run_gpu(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    import fluxos_cpp_b200 as fx
     n = args.size
     k_batch = args.in_flight  # steps per ADE launch
-    sc, h, conc = make_workload(n)
-    d = build_domain(sc, h, conc, k_batch)
+    sc = make_workload(n)
+    h, conc = sc.init_h, sc.init_conc[0]
     cells = n * n
-    d.step(args.warmup)
+    peak, peak_kind = _peaks()
+    gpu = gpu_id_of_device0()
+    precs = ["fp32", "fp64"] if args.precision == "both" else [args.precision]
+    doms, w0, res = {}, {}, {}
+    for p in precs:
+        doms[p] = build_domain(sc, k_batch, p)
+        w0[p] = doms[p].mass()[0]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    sampler = ClockSampler(gpu_id_of_device0())
-    sampler.start()
-    ms_total, ms_hydro, ms_ade = d.time_steps(args.steps)
-    clocks = sampler.stop()
+    for p in precs:
+        res[p] = measure_domain(doms[p], args.steps, args.warmup, cells, p, peak, gpu)
     torch.cuda.synchronize()
-    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+    head = precs[0]
+    t = torch.tensor([res[head]["ms_total"]], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
     ms_max = float(t.item())
-    st = d.status()
-    if st["device_error"]:
-        raise RuntimeError("device error during the timed steps")
     value = cells * args.steps * world / (ms_max / 1e3)
-    # dominant kernel and its roofline
-    peak, peak_kind = _peaks()
-    ms_h, ms_a = ms_hydro / args.steps, ms_ade / args.steps
-    kern = {"k_hydro": (ms_h, ALG_BYTES_HYDRO), "k_ade_sweep": (ms_a, ALG_BYTES_ADE)}
-    dom = max(kern, key=lambda k: kern[k][0])
-    dms, dbytes = kern[dom]
-    achieved = cells * dbytes / (dms / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get(f"{dom}_{n}")
-        except Exception:
-            traffic = None
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "traffic": traffic, "alg_bytes_per_cell": dbytes,
-                "ms_per_step": {"k_hydro": round(ms_h, 4), "k_ade_sweep": round(ms_a, 4)},
-                "ade_steps_per_launch": k_batch,
-                "step_alg_GBps": round(cells * ALG_BYTES_STEP / (ms_max / args.steps / 1e3) / 1e9, 1)}
+    acc = None
+    if len(precs) == 2:
+        acc = accuracy_of(doms["fp32"], doms["fp64"], w0["fp32"], w0["fp64"], sc.ks)
     e2e = None
     if not args.no_e2e:
-        secs, h2d, d2h = e2e_run(d, sc, args.steps)
+        secs, h2d, d2h = e2e_run(doms[head], sc, args.steps)
         e2e = {"value": cells * args.steps / secs, "unit": "cell-updates/s",
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                "note": "upload of the state from pinned host memory, K steps each reading its "
                        "status back, download of the Results fields; per-step bytes = totals / K"}
+    for d in doms.values():
+        d.close()
     batches = (args.steps + k_batch - 1) // k_batch
     launches = 2 * args.steps + 2 * batches  # finalize + hydro per step; batch open + sweep per batch
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_run(sc, h, conc, 1, args.cpu_steps, args.cpu_crop)
-    d.close()
+    mix = run_mix(args, peak) if (rank == 0 and world == 1 and not args.no_mix) else None
+    srv = run_serve(args) if (rank == 0 and world == 1 and not args.no_serve) else None
     if rank == 0:
+        roof = dict(res[head]["roofline"])
+        roof["peak_source"] = peak_kind
         line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if head == "fp32" else "f64",
                 "data": "synthetic (seeded fractal terrain, melt field and Manning n)",
                 "config": {"workload": f"fractal {n}x{n} cells of 2 m, 200 depressions, melt field "
                                        f"5-40 mm/day, Manning n U[0.03,0.15], one solute, wet start",
-                           "precision": "fp64 (parity path)", "cells": cells,
-                           "l2": "inputs larger than L2 (about 2 GB of state per replica)",
+                           "precision": head + (" (FP64 clock, wet/dry threshold tests and budget)"
+                                                if head == "fp32" else " (the reference's arithmetic)"),
+                           "cells": cells,
+                           "l2": "inputs larger than L2 (4-8 GB of state per replica)",
                            "parallelism": f"replicas x{world}"},
-                "roofline": roofline, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-                "cpu_baseline": cpu,
-                "accuracy": {"reference": "FP64 oracle, tests/test_gpu_parity.py",
-                             "max_rel_err_per_cell": "<= 1e-10"}}
+                "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res[head]["clocks"],
+                "cpu_baseline": cpu, "accuracy": acc}
+        if "fp64" in res and head != "fp64":
+            line["fp64"] = {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms_total"] / args.steps,
+                            "roofline": res["fp64"]["roofline"], "clocks": res["fp64"]["clocks"]}
+            line["fp32_over_fp64"] = round(res[head]["value"] / res["fp64"]["value"], 3)
+        if mix is not None:
+            line["mix"] = mix
+        if srv is not None:
+            line["serve"] = srv
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -325,7 +427,8 @@ def run_reference(args):
     if rank != 0:
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
-    sc, h, conc = make_workload(args.size)
+    sc = make_workload(args.size)
+    h, conc = sc.init_h, sc.init_conc[0]
     r = cpu_reference_run(sc, h, conc, args.warmup, args.steps, args.cpu_crop)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref is not built (the "
@@ -355,6 +458,14 @@ def main():
     ap.add_argument("--cpu-crop", type=int, default=2048)
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--in-flight", type=int, default=8, help="steps per ADE launch (1..15)")
+    ap.add_argument("--precision", default="both", choices=("both", "fp64", "fp32"),
+                    help="both: FP32 headline with FP64 beside it and the FP32 error")
+    ap.add_argument("--no-mix", action="store_true")
+    ap.add_argument("--mix-count", type=int, default=64)
+    ap.add_argument("--mix-steps", type=int, default=24)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 720.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -27,10 +27,15 @@ FIELDS = ("z", "zb", "h", "qx", "qy", "twet", "h0", "fe_1", "fe_2", "fe_3", "fn_
           "conc")
 
 # C header symbols, in declaration order (checked by tests/test_capi.py).
-EXPORTED = ("fx_create", "fx_destroy", "fx_last_error", "fx_device_bytes", "fx_upload", "fx_download",
+EXPORTED = ("fx_create", "fx_destroy", "fx_last_error", "fx_device_bytes", "fx_footprint", "fx_upload",
+            "fx_download",
             "fx_upload_flags", "fx_download_flags", "fx_set_forcing", "fx_set_manning",
             "fx_set_melt_field", "fx_set_option", "fx_prepare", "fx_step", "fx_run_to_print",
-            "fx_print_done", "fx_get_status", "fx_stream", "fx_time_steps", "fx_adesolver_noalloc",
+            "fx_print_done", "fx_get_status", "fx_stream", "fx_time_steps", "fx_mass", "fx_autotune",
+            "fx_batch_create",
+            "fx_batch_destroy", "fx_batch_last_error", "fx_batch_add", "fx_batch_remove",
+            "fx_batch_size", "fx_batch_step", "fx_batch_stream", "fx_batch_set_option",
+            "fx_batch_autotune", "fx_adesolver_noalloc",
             "fx_initiate",
             "fx_load_modset", "fx_open_modset", "fx_write_results", "fx_write_results_host", "fx_run")
 
@@ -52,14 +57,15 @@ class FxParams(C.Structure):
     _fields_ = [("hdry", C.c_double), ("ks", C.c_double), ("ntim", C.c_double),
                 ("print_step", C.c_double), ("print_next", C.c_double), ("tim", C.c_double),
                 ("h_min_print", C.c_double), ("ade", C.c_int), ("volrat_mode", C.c_int),
-                ("d_coef", C.c_double * MAX_CHEM), ("steps_in_flight", C.c_int)]
+                ("d_coef", C.c_double * MAX_CHEM), ("steps_in_flight", C.c_int),
+                ("precision", C.c_int)]
 
 
 class FxStatus(C.Structure):
     _fields_ = [("tim", C.c_double), ("dtfl", C.c_double), ("print_next", C.c_double),
                 ("hpall", C.c_double), ("steps", C.c_longlong), ("it", C.c_int),
                 ("print_pending", C.c_int), ("finished", C.c_int), ("device_error", C.c_int),
-                ("forcing_overrun", C.c_int)]
+                ("forcing_overrun", C.c_int), ("budget_melt", C.c_double), ("budget_out", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -84,6 +90,7 @@ def lib() -> C.CDLL:
     L.fx_last_error.argtypes = [vp]
     L.fx_last_error.restype = cp
     L.fx_device_bytes.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.fx_footprint.argtypes = [C.POINTER(FxGrid), C.POINTER(FxParams), ip, C.POINTER(C.c_longlong)]
     L.fx_upload.argtypes = [vp, cp, dp]
     L.fx_download.argtypes = [vp, cp, dp]
     L.fx_upload_flags.argtypes = [vp, fp, fp]
@@ -100,7 +107,22 @@ def lib() -> C.CDLL:
     L.fx_stream.argtypes = [vp]
     L.fx_stream.restype = vp
     L.fx_time_steps.argtypes = [vp, ip, dp, dp, dp]
+    L.fx_mass.argtypes = [vp, dp, dp]
+    L.fx_autotune.argtypes = [vp, ip, C.POINTER(ip)]
+    L.fx_batch_set_option.argtypes = [vp, cp, C.c_longlong]
+    L.fx_batch_autotune.argtypes = [vp, ip, C.POINTER(ip), C.POINTER(ip)]
     L.fx_adesolver_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, C.c_double, C.c_double, vp]
+    L.fx_batch_create.argtypes = [C.POINTER(vp)]
+    L.fx_batch_destroy.argtypes = [vp]
+    L.fx_batch_destroy.restype = None
+    L.fx_batch_last_error.argtypes = [vp]
+    L.fx_batch_last_error.restype = cp
+    L.fx_batch_add.argtypes = [vp, vp]
+    L.fx_batch_remove.argtypes = [vp, vp]
+    L.fx_batch_size.argtypes = [vp]
+    L.fx_batch_step.argtypes = [vp, ip, C.POINTER(FxStatus)]
+    L.fx_batch_stream.argtypes = [vp]
+    L.fx_batch_stream.restype = vp
     L.fx_initiate.argtypes = [vp, dp]
     L.fx_load_modset.argtypes = [cp, C.POINTER(FxGrid), C.POINTER(FxParams), dp, dp, dp, dp, dp, dp,
                                  dp, fp, fp, fp, C.POINTER(ip)]
@@ -169,6 +191,18 @@ def run(modset_path: str) -> None:
     _check(lib().fx_run(modset_path.encode()))
 
 
+def footprint(nrows: int, ncols: int, *, nchem: int = 1, precision: str = "fp64",
+              steps_in_flight: int = 0, extension_grids: int = 0) -> int:
+    """Device bytes a Domain of this size would hold (fx_footprint)."""
+    g = FxGrid(nrows, ncols, 1, nchem, -9999.0, 0.0, 0.0)
+    p = FxParams()
+    p.steps_in_flight = int(steps_in_flight)
+    p.precision = 1 if precision == "fp32" else 0
+    v = C.c_longlong(0)
+    _check(lib().fx_footprint(C.byref(g), C.byref(p), int(extension_grids), C.byref(v)))
+    return v.value
+
+
 class Domain:
     """One FLUXOS-OVERLAND domain resident on the GPU (an fx_ctx)."""
 
@@ -176,10 +210,14 @@ class Domain:
                  xll: float = 0.0, yll: float = 0.0, hdry: float = 0.001, ks: Optional[float] = None,
                  ntim: float = 0.0, print_step: float = 600.0, print_next: Optional[float] = None,
                  tim: float = 0.0, h_min_print: float = 0.0, ade: bool = True, volrat_mode: int = 0,
-                 d_coef: Sequence[float] = (0.01,), steps_in_flight: int = 0, _handle=None):
+                 d_coef: Sequence[float] = (0.01,), steps_in_flight: int = 0, precision: str = "fp64",
+                 _handle=None):
         self.L = lib()
         self.nrows, self.ncols, self.dxy, self.nchem = nrows, ncols, dxy, nchem
         self.xll, self.yll, self.h_min_print = xll, yll, h_min_print
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.precision = precision
         if _handle is not None:
             self.h = _handle
             return
@@ -197,6 +235,7 @@ class Domain:
         for k in range(MAX_CHEM):
             p.d_coef[k] = float(d_coef[k] if k < len(d_coef) else d_coef[-1])
         p.steps_in_flight = int(steps_in_flight)
+        p.precision = 1 if precision == "fp32" else 0
         h = C.c_void_p()
         _check(self.L.fx_create(C.byref(g), C.byref(p), C.byref(h)))
         self.h = h
@@ -309,5 +348,65 @@ class Domain:
         self._ck(self.L.fx_time_steps(self.h, int(n), C.byref(t), C.byref(a), C.byref(b)))
         return t.value, a.value, b.value
 
+    def autotune(self, trial_steps: int = 16) -> int:
+        """Pick the fastest tile shape on this domain (runs real steps)."""
+        r = C.c_int(0)
+        self._ck(self.L.fx_autotune(self.h, int(trial_steps), C.byref(r)))
+        return r.value
+
+    def mass(self):
+        """(stored water [m^3], array of stored solute masses), FP64 sums on the device."""
+        w = C.c_double()
+        m = np.zeros(MAX_CHEM)
+        self._ck(self.L.fx_mass(self.h, C.byref(w), _dptr(m)))
+        return w.value, m[: self.nchem].copy()
+
     def write_results(self, path: Optional[str] = None) -> None:
         self._ck(self.L.fx_write_results(self.h, path.encode() if path else None))
+
+
+class Batch:
+    """Several domains advanced together by the same launches (fx_batch)."""
+
+    def __init__(self):
+        self.L = lib()
+        h = C.c_void_p()
+        _check(self.L.fx_batch_create(C.byref(h)))
+        self.h = h
+        self.members = []
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.fx_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, d: "Domain") -> None:
+        _check(self.L.fx_batch_add(self.h, d.h))
+        self.members.append(d)
+
+    def remove(self, d: "Domain") -> None:
+        _check(self.L.fx_batch_remove(self.h, d.h))
+        self.members.remove(d)
+
+    def step(self, n: int) -> list:
+        arr = (FxStatus * max(1, len(self.members)))()
+        _check(self.L.fx_batch_step(self.h, int(n), arr))
+        return [arr[i].as_dict() for i in range(len(self.members))]
+
+    def stream(self) -> int:
+        return int(self.L.fx_batch_stream(self.h) or 0)
+
+    def set_option(self, name: str, value: int) -> None:
+        _check(self.L.fx_batch_set_option(self.h, name.encode(), int(value)))
+
+    def autotune(self, trial_steps: int = 8):
+        """(tile_rows, steps_in_flight) picked for this batch (runs real steps)."""
+        r, k = C.c_int(0), C.c_int(0)
+        _check(self.L.fx_batch_autotune(self.h, int(trial_steps), C.byref(r), C.byref(k)))
+        return r.value, k.value

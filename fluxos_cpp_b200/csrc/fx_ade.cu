@@ -37,6 +37,9 @@
 // is bounded and sets fx_ctl::error when it gives up.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "fx_common.cuh"
 
 namespace fxade {
@@ -50,28 +53,66 @@ constexpr long long SPIN_LIMIT = 1LL << 20;  // polls (well under a second) befo
 
 // Per-lane ring of prefetched cells, filled by cp.async (asynchronous
 // global -> shared copies).
+// T is the state's precision (double for the reference path, float for the
+// single-precision state).
+template <class T>
 struct Ring {
-  // the 16-byte aligned pair of concentrations holding this lane's cell: it
+  static constexpr int CV = 16 / sizeof(T);  // values per 16-byte copy
+  // the 16-byte aligned group of concentrations holding this lane's cell: it
   // is written during the launch by other warps, so it is copied with
   // cp.async.cg (L2 only; L1 is not coherent across SMs), which moves 16 bytes
-  double c[RING][32][2];
-  double h0[RING][32];   // depth after the melt, before the update
-  double h[RING][32];    // depth after the update
-  double hp[RING][32];   // depth before the step's melt
-  double mm[RING][32];   // melt-rate multiplier (1 without a melt field)
-  double fe1[RING][32];  // fe_1
-  double fn1[RING][32];  // fn_1
+  T c[RING][32][CV];
+  T h0[RING][32];   // depth after the melt, before the update
+  T h[RING][32];    // depth after the update
+  T hp[RING][32];   // depth before the step's melt
+  T mm[RING][32];   // melt-rate multiplier (1 without a melt field)
+  T fe1[RING][32];  // fe_1
+  T fn1[RING][32];  // fn_1
   unsigned fl[RING][32]; // the 4-byte word holding the cell's flag byte
 };
 
+template <class T>
 struct Rec {
-  double c;   // concentration before the sweep (after dilution, before re-scale)
-  double b;   // re-scaled concentration (ADEsolver_calc.cpp:64-72)
-  double h;   // depth after the hydrodynamic update
-  double qx;  // fe_1 of the cell
-  double qy;  // fn_1 of the cell
+  T c;   // concentration before the sweep (after dilution, before re-scale)
+  T b;   // re-scaled concentration (ADEsolver_calc.cpp:64-72)
+  T h;   // depth after the hydrodynamic update
+  T qx;  // fe_1 of the cell
+  T qy;  // fn_1 of the cell
   int ld;     // ldry (1 = dry); ghost cells read 0
 };
+
+// The state fields of the sweep in precision T.
+template <class T>
+struct Fields;
+template <>
+struct Fields<double> {
+  static __device__ __forceinline__ const double* h(const fx_dev& d) { return d.h; }
+  static __device__ __forceinline__ const double* h0(const fx_dev& d) { return d.h0; }
+  static __device__ __forceinline__ const double* hpm(const fx_dev& d) { return d.hpm; }
+  static __device__ __forceinline__ const double* fe1(const fx_dev& d) { return d.fe1; }
+  static __device__ __forceinline__ const double* fn1(const fx_dev& d) { return d.fn1; }
+  static __device__ __forceinline__ const double* mm(const fx_dev& d) { return d.melt_mult; }
+  static __device__ __forceinline__ double* conc(const fx_dev& d) { return d.conc; }
+};
+template <>
+struct Fields<float> {
+  static __device__ __forceinline__ const float* h(const fx_dev& d) { return d.h_f; }
+  static __device__ __forceinline__ const float* h0(const fx_dev& d) { return d.h0_f; }
+  static __device__ __forceinline__ const float* hpm(const fx_dev& d) { return d.hpm_f; }
+  static __device__ __forceinline__ const float* fe1(const fx_dev& d) { return d.fe1_f; }
+  static __device__ __forceinline__ const float* fn1(const fx_dev& d) { return d.fn1_f; }
+  static __device__ __forceinline__ const float* mm(const fx_dev& d) { return d.melt_mult_f; }
+  static __device__ __forceinline__ float* conc(const fx_dev& d) { return d.conc_f; }
+};
+
+template <class T>
+__device__ __forceinline__ T div_dxy(const fx_dev& d, T x) {
+  return d.dxy_pow2 ? x * (T)d.inv_dxy : x / (T)d.dxy;
+}
+template <class T>
+__device__ __forceinline__ T div_area(const fx_dev& d, T x) {
+  return d.dxy_pow2 ? x * (T)d.inv_area : x / (T)d.arbase;
+}
 
 // The step a unit works on.
 struct StepIn {
@@ -85,6 +126,12 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool val
   const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
   const int n = valid ? 8 : 0;  // 0 source bytes: the slot is zero-filled
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+}
+template <int B>
+__device__ __forceinline__ void cp_async_n(void* smem, const void* gmem, bool valid) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? B : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(gmem), "n"(B), "r"(n) : "memory");
 }
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {
   const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
@@ -103,20 +150,23 @@ __device__ __forceinline__ void cp_wait() {
 }
 
 // Issue the copies of cell (ix, iy) into ring slot `slot` of this lane.
-__device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const double* A, Ring& R, int lane,
+template <class T>
+__device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const T* A, Ring<T>& R, int lane,
                                          int ix, int iy) {
+  using F = Fields<T>;
+  constexpr int B = sizeof(T);
   const int slot = iy & (RING - 1);
   const bool inr = ix >= 0 && ix <= d.nr + 1 && iy >= 0 && iy <= d.nc + 1;
   const long long gi = inr ? fx_ix(d, ix, iy) : 0;
-  cp_async16_cg(&R.c[slot][lane][0], A + (gi & ~1LL), inr);
-  cp_async8(&R.h0[slot][lane], d.h0 + S.cur + gi, inr);
-  cp_async8(&R.h[slot][lane], d.h + S.cur + gi, inr);
-  cp_async8(&R.hp[slot][lane], S.dilute ? (const void*)(d.hpm + S.cur + gi) : (const void*)d.h,
-            inr && S.dilute);
-  const bool mm_ok = inr && S.dilute && d.melt_mult != nullptr;
-  cp_async8(&R.mm[slot][lane], mm_ok ? (const void*)(d.melt_mult + gi) : (const void*)d.h, mm_ok);
-  cp_async8(&R.fe1[slot][lane], d.fe1 + S.cur + gi, inr);
-  cp_async8(&R.fn1[slot][lane], d.fn1 + S.cur + gi, inr);
+  cp_async16_cg(&R.c[slot][lane][0], A + (gi & ~(long long)(Ring<T>::CV - 1)), inr);
+  cp_async_n<B>(&R.h0[slot][lane], F::h0(d) + S.cur + gi, inr);
+  cp_async_n<B>(&R.h[slot][lane], F::h(d) + S.cur + gi, inr);
+  cp_async_n<B>(&R.hp[slot][lane], S.dilute ? (const void*)(F::hpm(d) + S.cur + gi) : (const void*)F::h(d),
+                inr && S.dilute);
+  const bool mm_ok = inr && S.dilute && F::mm(d) != nullptr;
+  cp_async_n<B>(&R.mm[slot][lane], mm_ok ? (const void*)(F::mm(d) + gi) : (const void*)F::h(d), mm_ok);
+  cp_async_n<B>(&R.fe1[slot][lane], F::fe1(d) + S.cur + gi, inr);
+  cp_async_n<B>(&R.fn1[slot][lane], F::fn1(d) + S.cur + gi, inr);
   cp_async4(&R.fl[slot][lane], d.flags + S.cur + (gi & ~3LL), inr);
 }
 
@@ -124,14 +174,15 @@ __device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const
 // (common.cpp:214-234) when the step has one, then the re-scale of
 // ADEsolver_calc.cpp:64-72 when the step sweeps. Ghost cells carry only their
 // depth (their concentration is 0 and never changes).
-__device__ __forceinline__ Rec make_rec(const fx_dev& d, const StepIn& S, const Ring& R, int lane, int ix,
-                                        int iy) {
-  Rec r;
-  r.c = 0.0;
-  r.b = 0.0;
-  r.h = 0.0;
-  r.qx = 0.0;
-  r.qy = 0.0;
+template <class T>
+__device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, const Ring<T>& R, int lane, int ix,
+                                           int iy) {
+  Rec<T> r;
+  r.c = T(0);
+  r.b = T(0);
+  r.h = T(0);
+  r.qx = T(0);
+  r.qy = T(0);
   r.ld = 0;
   if (ix < 0 || ix > d.nr + 1 || iy < 0 || iy > d.nc + 1) return r;
   const int slot = iy & (RING - 1);
@@ -141,20 +192,21 @@ __device__ __forceinline__ Rec make_rec(const fx_dev& d, const StepIn& S, const 
     const unsigned fl = (R.fl[slot][lane] >> (8 * (unsigned)(gi & 3))) & 0xffu;
     r.ld = fl & FX_F_LDRY;
     const int ldp = (fl & FX_F_LDRY_PREV) ? 1 : 0;
-    double c = R.c[slot][lane][gi & 1];
-    const double h0 = R.h0[slot][lane];
+    T c = R.c[slot][lane][gi & (Ring<T>::CV - 1)];
+    const T h0 = R.h0[slot][lane];
     if (S.dilute && !(fl & FX_F_NODATA)) {
-      const double hp = R.hp[slot][lane];
-      if (hp != 0.0) {
-        const double mi =
-            d.melt_mult ? (double)S.meteo_rate * R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt : S.meteoi;
-        c = (c * hp + (mi * S.mconc)) / (h0);
+      const T hp = R.hp[slot][lane];
+      if (hp != T(0)) {
+        const T mi = Fields<T>::mm(d)
+                         ? (T)((double)S.meteo_rate * (double)R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
+                         : (T)S.meteoi;
+        c = (c * hp + (mi * (T)S.mconc)) / (h0);
       }
     }
     r.c = c;
     if (!S.sweep) r.b = c;
     else if (r.ld == 0 && ldp == 0) r.b = c * h0 / r.h;
-    else if (r.ld == 1) r.b = 0.0;
+    else if (r.ld == 1) r.b = T(0);
     else r.b = c;
     r.qx = R.fe1[slot][lane];
     r.qy = R.fn1[slot][lane];
@@ -162,9 +214,12 @@ __device__ __forceinline__ Rec make_rec(const fx_dev& d, const StepIn& S, const 
   return r;
 }
 
-__device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
-__device__ __forceinline__ double shdn(double v, int k) { return __shfl_down_sync(0xffffffffu, v, k); }
-__device__ __forceinline__ double shup(double v, int k) { return __shfl_up_sync(0xffffffffu, v, k); }
+template <class V>
+__device__ __forceinline__ V shfl_d(V v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <class V>
+__device__ __forceinline__ V shdn(V v, int k) { return __shfl_down_sync(0xffffffffu, v, k); }
+template <class V>
+__device__ __forceinline__ V shup(V v, int k) { return __shfl_up_sync(0xffffffffu, v, k); }
 
 __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
   unsigned long long v;
@@ -176,103 +231,103 @@ __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long 
 }
 
 // One cell of the sweep, ADEsolver_calc.cpp:126-288, for a wet cell.
-__device__ __forceinline__ void ade_cell(const fx_dev& d, double D, double dt, bool last_row,
-                                         bool last_col, double hp, double he, double hn, double qxl,
-                                         double qyl, double fw, double fp, double fe, double fee,
-                                         double fs, double fn, double fnn, double pfw, double qfs,
-                                         int ldE, int ldW, int ldEE, int ldN, int ldS, int ldNN,
-                                         double cmax, double cmin, double& con, double& pfe_out,
-                                         double& qfn_out) {
-  const double nt = 1;
-  const double dx = d.dxy, dy = d.dxy;
-  const double area = d.arbase, areae = d.arbase, arean = d.arbase;
-  const double ntp = nt;
-  double fem, pfde, hnue, hne;
+// T = double is the reference's arithmetic; T = float the single-precision
+// state's (same operations, same order).
+template <class T>
+__device__ __forceinline__ void ade_cell(const fx_dev& d, T D, T dt, bool last_row, bool last_col, T hp,
+                                         T he, T hn, T qxl, T qyl, T fw, T fp, T fe, T fee, T fs, T fn,
+                                         T fnn, T pfw, T qfs, int ldE, int ldW, int ldEE, int ldN, int ldS,
+                                         int ldNN, T cmax, T cmin, T& con, T& pfe_out, T& qfn_out) {
+  const T nt = 1;
+  const T dx = (T)d.dxy, dy = (T)d.dxy;
+  const T area = (T)d.arbase, areae = (T)d.arbase, arean = (T)d.arbase;
+  const T ntp = nt;
+  T fem, pfde, hnue, hne;
   if (ldE == 0) {  // :151-172
-    hnue = fmax(hp * nt * he * nt, .0001);
-    hne = fx_div_dxy(d, sqrt(hnue) * 2.0) * dy * D;  // sigc = 0.5: /sigc is *2 exactly
+    hnue = fmax(hp * nt * he * nt, T(.0001));
+    hne = div_dxy<T>(d, sqrt(hnue) * T(2)) * dy * D;  // sigc = 0.5: /sigc is *2 exactly
     pfde = -hne * (fe - fp);
-    if (qxl > 0.0) {
-      if (ldW == 0) fem = -.125 * fw + .75 * fp + .375 * fe;
-      else fem = 0.5 * fp + 0.5 * fe;
+    if (qxl > T(0)) {
+      if (ldW == 0) fem = T(-.125) * fw + T(.75) * fp + T(.375) * fe;
+      else fem = T(.5) * fp + T(.5) * fe;
     } else {
-      if (ldEE == 0) fem = .375 * fp + .75 * fe - .125 * fee;
-      else fem = 0.5 * fp + 0.5 * fe;
+      if (ldEE == 0) fem = T(.375) * fp + T(.75) * fe - T(.125) * fee;
+      else fem = T(.5) * fp + T(.5) * fe;
     }
   } else {
-    fem = 0.;
-    pfde = 0.;
+    fem = T(0);
+    pfde = T(0);
   }
-  fem = fmax(0., fem);
-  if (last_row) fem = 0.0;  // :176-178, ghost concentration c(NROWS+1, iy) = 0
-  const double pfce = qxl * fem * dy;
-  double pfe = pfce + pfde;
-  if (pfe < 0) {  // :187-194
+  fem = fmax(T(0), fem);
+  if (last_row) fem = T(0);  // :176-178, ghost concentration c(NROWS+1, iy) = 0
+  const T pfce = qxl * fem * dy;
+  T pfe = pfce + pfde;
+  if (pfe < T(0)) {  // :187-194
     if (ldE == 0) {
-      const double cvolrate = -(fe * he) * areae / dt;
+      const T cvolrate = -(fe * he) * areae / dt;
       pfe = fmax(pfe, cvolrate);
     } else {
-      pfe = 0.;
+      pfe = T(0);
     }
   }
-  double fnm, qfdn, hnn;
+  T fnm, qfdn, hnn;
   if (ldN == 0) {  // :198-218
-    hnue = fmax(.0001, hp * ntp * hn * nt);
-    hnn = fx_div_dxy(d, sqrt(hnue) * 2.0) * dx * D;
+    hnue = fmax(T(.0001), hp * ntp * hn * nt);
+    hnn = div_dxy<T>(d, sqrt(hnue) * T(2)) * dx * D;
     qfdn = -hnn * (fn - fp);
-    if (qyl > 0.0) {
-      if (ldS == 0) fnm = -.125 * fs + .75 * fp + .375 * fn;
-      else fnm = 0.5 * fp + .5 * fn;
+    if (qyl > T(0)) {
+      if (ldS == 0) fnm = T(-.125) * fs + T(.75) * fp + T(.375) * fn;
+      else fnm = T(.5) * fp + T(.5) * fn;
     } else {
-      if (ldNN == 0) fnm = .375 * fp + .75 * fn - .125 * fnn;
-      else fnm = .5 * fp + .5 * fn;
+      if (ldNN == 0) fnm = T(.375) * fp + T(.75) * fn - T(.125) * fnn;
+      else fnm = T(.5) * fp + T(.5) * fn;
     }
   } else {
-    fnm = 0.;
-    qfdn = 0.;
+    fnm = T(0);
+    qfdn = T(0);
   }
-  fnm = fmax(0., fnm);
-  if (last_col) fnm = 0.0;  // :223-225, ghost concentration c(ix, NCOLS+1) = 0
-  const double qfcn = qyl * fnm * dx;
-  double qfn = qfcn + qfdn;
-  if (qfn < 0) {  // :234-241
+  fnm = fmax(T(0), fnm);
+  if (last_col) fnm = T(0);  // :223-225, ghost concentration c(ix, NCOLS+1) = 0
+  const T qfcn = qyl * fnm * dx;
+  T qfn = qfcn + qfdn;
+  if (qfn < T(0)) {  // :234-241
     if (ldN == 0) {
-      const double cvolrate = -(fn * hn) * arean / dt;
+      const T cvolrate = -(fn * hn) * arean / dt;
       qfn = fmax(qfn, cvolrate);
     } else {
-      qfn = 0.;
+      qfn = T(0);
     }
   }
-  const double cvolpot = (fp * hp) * area;  // :243-278
-  const double cvolrat = cvolpot / dt + pfw + qfs;
-  if (cvolrat > 0.0) {
-    if (pfe > 0. && qfn > 0.) {
+  const T cvolpot = (fp * hp) * area;  // :243-278
+  const T cvolrat = cvolpot / dt + pfw + qfs;
+  if (cvolrat > T(0)) {
+    if (pfe > T(0) && qfn > T(0)) {
       if (pfe + qfn > cvolrat) {
-        const double cf = qfn / (pfe + qfn);
-        pfe = (1. - cf) * cvolrat;
+        const T cf = qfn / (pfe + qfn);
+        pfe = (T(1) - cf) * cvolrat;
         qfn = cf * cvolrat;
       }
-    } else if (pfe > 0.) {
+    } else if (pfe > T(0)) {
       pfe = fmin(pfe, (cvolrat - qfn));
-    } else if (qfn > 0.) {
+    } else if (qfn > T(0)) {
       qfn = fmin(qfn, (cvolrat - pfe));
     }
   } else {
-    if (pfe >= 0. && qfn < 0.) {
-      const double cbilan = cvolrat - qfn;
-      if (cbilan > 0.) pfe = fmin(pfe, cbilan);
-      else pfe = 0.;
-    } else if (pfe < 0. && qfn >= 0.) {
-      const double cbilan = cvolrat - pfe;
-      if (cbilan > 0.) qfn = fmin(qfn, cbilan);
-      else qfn = 0.;
-    } else if (pfe >= 0. && qfn >= 0.) {
-      pfe = 0.0;
-      qfn = 0.0;
+    if (pfe >= T(0) && qfn < T(0)) {
+      const T cbilan = cvolrat - qfn;
+      if (cbilan > T(0)) pfe = fmin(pfe, cbilan);
+      else pfe = T(0);
+    } else if (pfe < T(0) && qfn >= T(0)) {
+      const T cbilan = cvolrat - pfe;
+      if (cbilan > T(0)) qfn = fmin(qfn, cbilan);
+      else qfn = T(0);
+    } else if (pfe >= T(0) && qfn >= T(0)) {
+      pfe = T(0);
+      qfn = T(0);
     }
   }
-  const double dc = fx_div_area(d, (pfw - pfe + qfs - qfn) * dt);  // :281-286
-  double cn = fp + dc / hp;
+  const T dc = div_area<T>(d, (pfw - pfe + qfs - qfn) * dt);  // :281-286
+  T cn = fp + dc / hp;
   cn = fmin(cmax, cn);
   cn = fmax(cmin, cn);
   con = cn;
@@ -319,46 +374,29 @@ __device__ __forceinline__ bool wait_deps(const fx_dev& d, Deps& D, int need_w, 
   }
 }
 
-__global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ int s_nj;
-  __shared__ int s_slot[FX_MAX_SLOTS];
-  const fx_ctl& cc = *d.ctl;
-  if (!d.ade) return;
-  if (threadIdx.x == 0) {
-    // this batch's live steps, in step order
-    int n = 0;
-    for (int k = 0; k < d.nslot; ++k) {
-      const fx_steprec& r = cc.rec[k];
+// Sweep of one unit: strip s of solute k at the jj-th live step of the batch.
+// Returns false when a wait gave up.
+template <class T>
+__device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, int k, int s, int lane) {
+  {
+    const fx_ctl& cc = *d.ctl;
+    // this batch's live steps are consecutive: the jj-th is minstep + jj
+    int m = 0;
+    long long minstep = 0;
+    for (int q = 0; q < d.nslot; ++q) {
+      const fx_steprec& r = cc.rec[q];
       if (r.live && r.batch == cc.batch) {
-        int j = n++;
-        while (j > 0 && cc.rec[s_slot[j - 1]].step > r.step) {
-          s_slot[j] = s_slot[j - 1];
-          --j;
-        }
-        s_slot[j] = k;
+        minstep = (m == 0 || r.step < minstep) ? r.step : minstep;
+        ++m;
       }
     }
-    s_nj = n;
-  }
-  __syncthreads();
-  const int nj = s_nj;
-  if (nj == 0) return;
-  const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  Ring& R = reinterpret_cast<Ring*>(smem_raw)[wib];
-  const int wg = blockIdx.x * WARPS + wib;
-  const int nwarps = gridDim.x * WARPS;
-  const int per_step = nstrips * d.nchem;
-  const int units = nj * per_step;
-  const int T = d.nc + ROWS - 1;  // warp steps per strip
-  const long long bnd_stride = (long long)(d.nc + 2) * 3;
-  auto unit_index = [&](int slot, int k, int s) { return ((long long)slot * d.nchem + k) * nstrips + s; };
-
-  for (int u = wg; u < units; u += nwarps) {
-    const int jj = u / per_step, rem = u % per_step;
-    const int k = rem / nstrips, s = rem % nstrips;
-    const int slot = s_slot[jj];
+    if (jj >= m) return true;
+    const long long step = minstep + jj;
+    const int slot = (int)(step % d.nslot);
+    const int nstrips = (d.nr + ROWS - 1) / ROWS;
+    const int TW = d.nc + ROWS - 1;  // warp steps per strip
+    const long long bnd_stride = (long long)(d.nc + 2) * 3;
+    auto unit_index = [&](int sl, int kk, int ss) { return ((long long)sl * d.nchem + kk) * nstrips + ss; };
     const fx_steprec& rec = cc.rec[slot];
     const unsigned long long tag = (unsigned long long)rec.step;
     StepIn S;
@@ -369,15 +407,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
     S.dt = rec.dtfl;
     S.sweep = rec.active && rec.it > 1;  // :45,74-77
     S.dilute = d.has_meteo != 0;
-    double* A = d.conc + k * d.plane;
-    const double D = d.dcoef[k];
+    T* A = Fields<T>::conc(d) + k * d.plane;
+    const T D = (T)d.dcoef[k];
     const int ix0 = 1 + s * ROWS;
     const int ix = ix0 + lane;
     const bool compute_lane = lane < ROWS && ix <= d.nr;
     // dependencies: the west strip of this step, this strip and the next
     // strip of the previous step of the batch (earlier batches are complete)
     const unsigned long long* prog_w = (s > 0) ? d.ade_prog + unit_index(slot, k, s - 1) : nullptr;
-    const int pslot = jj > 0 ? s_slot[jj - 1] : -1;
+    const int pslot = (int)((step - 1) % d.nslot);
     const unsigned long long* prog_p0 = jj > 0 ? d.ade_prog + unit_index(pslot, k, s) : nullptr;
     const unsigned long long* prog_p1 =
         (jj > 0 && s + 1 < nstrips) ? d.ade_prog + unit_index(pslot, k, s + 1) : nullptr;
@@ -395,43 +433,43 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
     // the previous step must have written every column prefetched before a
     // check (lanes 0..29 of its strip s, lanes 0..1 of its strip s + 1), and
     // the west strip of this step the boundary columns read in the chunk
-    auto need_p0 = [&](int col) { return min(col + ROWS, T); };
-    auto need_p1 = [&](int col) { return min(col + 2, T); };
-    if (!wait_deps(d, dep, min(CHUNK - 1 + ROWS, T), need_p0(DIST + 3), need_p1(DIST + 3))) bail = true;
+    auto need_p0 = [&](int col) { return min(col + ROWS, TW); };
+    auto need_p1 = [&](int col) { return min(col + 2, TW); };
+    if (!wait_deps(d, dep, min(CHUNK - 1 + ROWS, TW), need_p0(DIST + 3), need_p1(DIST + 3))) bail = true;
 
     // prime the ring: columns iy0 .. iy0 + DIST + 2 of this lane's row
     const int iy0 = 1 - lane;
     if (!bail) {
       for (int j = 0; j < DIST + 3; ++j) {
-        prefetch(d, S, A, R, lane, ix, iy0 + j);
+        prefetch<T>(d, S, A, R, lane, ix, iy0 + j);
         cp_commit();
       }
     }
     cp_wait<0>();
-    Rec cur = make_rec(d, S, R, lane, ix, iy0);
-    Rec n1 = make_rec(d, S, R, lane, ix, iy0 + 1);
-    Rec n2 = make_rec(d, S, R, lane, ix, iy0 + 2);
+    Rec<T> cur = make_rec<T>(d, S, R, lane, ix, iy0);
+    Rec<T> n1 = make_rec<T>(d, S, R, lane, ix, iy0 + 1);
+    Rec<T> n2 = make_rec<T>(d, S, R, lane, ix, iy0 + 2);
     // carries: outputs of this lane's previous cell (its south cell for the
     // next step, its west cell for lane + 1)
-    double o_c = 0.0, o_pfe = 0.0, o_b = 0.0, o_qfn = 0.0;
+    T o_c = T(0), o_pfe = T(0), o_b = T(0), o_qfn = T(0);
     int o_ld = 0;
     // west-boundary values of the current and the next chunk (lane j holds
     // column chunk_start + 1 + j); strip 0's west neighbour is the ghost row 0:
     // c = 0, pfe = the ghost convective flux c(0,iy)*fe_1(0,iy)*dy = 0 (:106-116)
-    double bw_c = 0.0, bw_pfe = 0.0, bw_b = 0.0, bn_c = 0.0, bn_pfe = 0.0, bn_b = 0.0;
+    T bw_c = T(0), bw_pfe = T(0), bw_b = T(0), bn_c = T(0), bn_pfe = T(0), bn_b = T(0);
     int bw_ld = 0, bn_ld = 0;
     if (!bail && prog_w) {
       const int iyb = 1 + lane;
       if (lane < CHUNK && iyb <= d.nc) {
         const double* p = bnd_in + (long long)iyb * 3;
-        bn_c = __ldcg(p);
-        bn_pfe = __ldcg(p + 1);
-        bn_b = __ldcg(p + 2);
+        bn_c = (T)__ldcg(p);
+        bn_pfe = (T)__ldcg(p + 1);
+        bn_b = (T)__ldcg(p + 2);
         bn_ld = d.flags[S.cur + fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
       }
     }
 
-    for (int tau = 0; tau < T && !bail; ++tau) {
+    for (int tau = 0; tau < TW && !bail; ++tau) {
       if ((tau % CHUNK) == 0) {
         bw_c = bn_c;
         bw_pfe = bn_pfe;
@@ -440,19 +478,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
         // columns lane 0 prefetches during this chunk, and the next chunk's
         // boundary (loaded now, used in CHUNK steps)
         const int col = tau + CHUNK + DIST + 3;
-        if (!wait_deps(d, dep, min(tau + 2 * CHUNK - 1 + ROWS, T), need_p0(col), need_p1(col))) {
+        if (!wait_deps(d, dep, min(tau + 2 * CHUNK - 1 + ROWS, TW), need_p0(col), need_p1(col))) {
           bail = true;
           break;
         }
-        if (prog_w && tau + CHUNK < T) {
+        if (prog_w && tau + CHUNK < TW) {
           const int iyb = tau + CHUNK + 1 + lane;
-          bn_c = bn_pfe = bn_b = 0.0;
+          bn_c = bn_pfe = bn_b = T(0);
           bn_ld = 0;
           if (lane < CHUNK && iyb <= d.nc) {
             const double* p = bnd_in + (long long)iyb * 3;
-            bn_c = __ldcg(p);
-            bn_pfe = __ldcg(p + 1);
-            bn_b = __ldcg(p + 2);
+            bn_c = (T)__ldcg(p);
+            bn_pfe = (T)__ldcg(p + 1);
+            bn_b = (T)__ldcg(p + 2);
             bn_ld = d.flags[S.cur + fx_ix(d, ix0 - 1, iyb)] & FX_F_LDRY;
           }
         }
@@ -460,19 +498,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
       const int iy = tau - lane + 1;
       // keep DIST columns in flight: column iy + DIST + 3 now, column iy + 3
       // must have landed by the end of this step
-      prefetch(d, S, A, R, lane, ix, iy + DIST + 3);
+      prefetch<T>(d, S, A, R, lane, ix, iy + DIST + 3);
       cp_commit();
       // east (lane+1's next column), east-east (lane+2's column after next)
-      const double E_c = shdn(n1.c, 1), E_b = shdn(n1.b, 1), E_h = shdn(n1.h, 1);
+      const T E_c = shdn(n1.c, 1), E_b = shdn(n1.b, 1), E_h = shdn(n1.h, 1);
       const int E_ld = __shfl_down_sync(0xffffffffu, n1.ld, 1);
-      double EE_b = shdn(n2.b, 2);
+      T EE_b = shdn(n2.b, 2);
       int EE_ld = __shfl_down_sync(0xffffffffu, n2.ld, 2);
       // west: lane-1's outputs of the previous step, or the boundary
-      double W_c = shup(o_c, 1), W_pfe = shup(o_pfe, 1), W_b = shup(o_b, 1);
+      T W_c = shup(o_c, 1), W_pfe = shup(o_pfe, 1), W_b = shup(o_b, 1);
       int W_ld = __shfl_up_sync(0xffffffffu, o_ld, 1);
       {
         const int j = tau % CHUNK;
-        const double t_c = shfl_d(bw_c, j), t_pfe = shfl_d(bw_pfe, j), t_b = shfl_d(bw_b, j);
+        const T t_c = shfl_d(bw_c, j), t_pfe = shfl_d(bw_pfe, j), t_b = shfl_d(bw_b, j);
         const int t_ld = __shfl_sync(0xffffffffu, bw_ld, j);
         if (lane == 0) {
           W_c = t_c;
@@ -484,30 +522,30 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
       if (compute_lane && iy >= 1 && iy <= d.nc) {
         const long long gi = fx_ix(d, ix, iy);
         const bool last_row = ix == d.nr, last_col = iy == d.nc;
-        double out_c, pfe = 0.0, qfn = 0.0;
+        T out_c, pfe = T(0), qfn = T(0);
         if (last_row) {  // iee = min(ix+2, NROWS+1) = ie
           EE_b = E_b;
           EE_ld = E_ld;
         }
-        const double NN_b = last_col ? n1.b : n2.b;  // inn = min(iy+2, NCOLS+1)
+        const T NN_b = last_col ? n1.b : n2.b;  // inn = min(iy+2, NCOLS+1)
         const int NN_ld = last_col ? n1.ld : n2.ld;
         if (!S.sweep || (last_row && last_col)) {
           out_c = cur.b;  // no sweep this step, or the cell the sweep stops short of (:93)
         } else if (cur.ld == 1) {
-          out_c = 0.0;  // :119-124
+          out_c = T(0);  // :119-124
         } else {
-          const double cmax = fmax(W_b, fmax(E_c, fmax(o_b, n1.c)));
-          const double cmin = fmin(W_b, fmin(E_c, fmin(o_b, n1.c)));
-          ade_cell(d, D, S.dt, last_row, last_col, cur.h, E_h, n1.h, cur.qx, cur.qy, W_c, cur.b, E_b,
+          const T cmax = fmax(W_b, fmax(E_c, fmax(o_b, n1.c)));
+          const T cmin = fmin(W_b, fmin(E_c, fmin(o_b, n1.c)));
+          ade_cell<T>(d, D, (T)S.dt, last_row, last_col, cur.h, E_h, n1.h, cur.qx, cur.qy, W_c, cur.b, E_b,
                    EE_b, o_c, n1.b, NN_b, W_pfe, o_qfn, E_ld, W_ld, EE_ld, n1.ld, o_ld, NN_ld, cmax,
                    cmin, out_c, pfe, qfn);
         }
         A[gi] = out_c;
         if (lane == ROWS - 1 && bnd_out) {
           double* p = bnd_out + (long long)iy * 3;
-          p[0] = out_c;
-          p[1] = pfe;
-          p[2] = cur.b;
+          p[0] = (double)out_c;
+          p[1] = (double)pfe;
+          p[2] = (double)cur.b;
         }
         o_c = out_c;
         o_pfe = pfe;
@@ -516,18 +554,18 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
         o_qfn = qfn;
       } else if (iy < 1) {
         // not started: the south neighbour of column 1 is the ghost column
-        o_c = 0.0;
-        o_pfe = 0.0;
-        o_b = 0.0;
+        o_c = T(0);
+        o_pfe = T(0);
+        o_b = T(0);
         o_ld = 0;
-        o_qfn = 0.0;
+        o_qfn = T(0);
       }
       // publish progress: every lane's writes of this chunk, then the count.
       // The next strip of this step overwrites its first two rows only after
       // this count passes the column by ROWS steps; lanes 30 and 31 copied
       // those rows DIST + 3 columns ahead, and cp_wait below retires a copy
       // DIST steps after it was issued, so the copies have landed by then.
-      if (((tau + 1) % CHUNK) == 0 || tau + 1 == T) {
+      if (((tau + 1) % CHUNK) == 0 || tau + 1 == TW) {
         __threadfence();
         __syncwarp();
         if (lane == 0) st_release(prog_me, (tag << 32) | (unsigned)(tau + 1));
@@ -535,10 +573,55 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
       cp_wait<DIST>();
       cur = n1;
       n1 = n2;
-      n2 = make_rec(d, S, R, lane, ix, iy + 3);
+      n2 = make_rec<T>(d, S, R, lane, ix, iy + 3);
     }
     cp_wait<0>();
-    if (bail) return;
+    return !bail;
+  }
+}
+
+// One domain: the descriptor is a kernel parameter. Unit u is strip
+// u % nstrips of solute (u / nstrips) % nchem at step u / (nstrips * nchem).
+template <class T>
+__global__ void __launch_bounds__(WARPS * 32) k_ade_one(const __grid_constant__ fx_dev d, int nunits) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  Ring<T>& R = reinterpret_cast<Ring<T>*>(smem_raw)[wib];
+  const int nwarps = gridDim.x * WARPS;
+  if (!d.ade) return;
+  const int nstrips = (d.nr + ROWS - 1) / ROWS;
+  for (int u = blockIdx.x * WARPS + wib; u < nunits; u += nwarps) {
+    const int s = u % nstrips, k = (u / nstrips) % d.nchem, jj = u / (nstrips * d.nchem);
+    if (!ade_unit<T>(d, R, jj, k, s, lane)) return;
+  }
+}
+
+// A batch of domains: units come from the unit table; each warp copies its
+// unit's descriptor to its own shared-memory slot.
+template <class T>
+__global__ void __launch_bounds__(WARPS * 32) k_ade_batch(const fx_dev* __restrict__ devs,
+                                                         const fx_unit* __restrict__ units, int nunits) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ fx_dev wdev[WARPS];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  Ring<T>& R = reinterpret_cast<Ring<T>*>(smem_raw)[wib];
+  const int nwarps = gridDim.x * WARPS;
+  int have = -1;
+  for (int u = blockIdx.x * WARPS + wib; u < nunits; u += nwarps) {
+    const fx_unit un = units[u];
+    if (un.dom != have) {
+      __syncwarp();
+      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(devs + un.dom);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(&wdev[wib]);
+      for (int i = lane; i < (int)(sizeof(fx_dev) / 8); i += 32) dst[i] = src[i];
+      __syncwarp();
+      have = un.dom;
+    }
+    const fx_dev& d = wdev[wib];
+    if (!d.ade) continue;
+    if (!ade_unit<T>(d, R, un.jj, un.k, un.s, lane)) return;
   }
 }
 
@@ -546,22 +629,50 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_sweep(fx_dev d, int nstrips)
 
 int fx_ade_rows_per_strip() { return fxade::ROWS; }
 int fx_ade_threads_per_block() { return fxade::WARPS * 32; }
-static const size_t kAdeSmem = sizeof(fxade::Ring) * fxade::WARPS;
-
-void fx_launch_ade(const fx_dev& d, int nstrips, int nblocks, cudaStream_t s) {
-  fxade::k_ade_sweep<<<nblocks, fxade::WARPS * 32, kAdeSmem, s>>>(d, nstrips);
+static size_t ade_smem(bool prec32) {
+  return (prec32 ? sizeof(fxade::Ring<float>) : sizeof(fxade::Ring<double>)) * fxade::WARPS;
 }
 
-int fx_ade_max_blocks(int* out) {
-  int dev = 0, nsm = 0, per = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
-  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-  if (cudaFuncSetAttribute(fxade::k_ade_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdeSmem) !=
-      cudaSuccess)
-    return -1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fxade::k_ade_sweep, fxade::WARPS * 32, kAdeSmem) !=
-      cudaSuccess)
+void fx_launch_ade(const fx_dev* devs, const fx_unit* units, int nunits, int nblocks, bool prec32, cudaStream_t s) {
+  if (prec32) fxade::k_ade_batch<float><<<nblocks, fxade::WARPS * 32, ade_smem(true), s>>>(devs, units, nunits);
+  else fxade::k_ade_batch<double><<<nblocks, fxade::WARPS * 32, ade_smem(false), s>>>(devs, units, nunits);
+}
+void fx_launch_ade_one(const fx_dev& d, int nunits, int nblocks, cudaStream_t s) {
+  if (d.prec32) fxade::k_ade_one<float><<<nblocks, fxade::WARPS * 32, ade_smem(true), s>>>(d, nunits);
+  else fxade::k_ade_one<double><<<nblocks, fxade::WARPS * 32, ade_smem(false), s>>>(d, nunits);
+}
+
+// Appends the ADE units of domain `dom` for a batch of `steps` steps, in the
+// order their dependencies require (step, then solute, then strip).
+void fx_units_of(int dom, int nr, int nchem, int steps, std::vector<fx_unit>& out) {
+  const int nstrips = (nr + fxade::ROWS - 1) / fxade::ROWS;
+  for (int jj = 0; jj < steps; ++jj)
+    for (int k = 0; k < nchem; ++k)
+      for (int s = 0; s < nstrips; ++s) out.push_back(fx_unit{dom, jj, k, s});
+}
+
+template <class K>
+static int max_blocks_of(K kernel, size_t smem, int nsm, int* out) {
+  int per = 0;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, fxade::WARPS * 32, smem) != cudaSuccess)
     return -1;
   *out = per * nsm;
+  return 0;
+}
+
+// Resident blocks of the sweep kernels on this device (the smallest of the
+// four variants), after raising their dynamic shared memory limit.
+int fx_ade_max_blocks(int* out) {
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+  int a = 0, b = 0, c = 0, e = 0;
+  if (max_blocks_of(fxade::k_ade_one<double>, ade_smem(false), nsm, &a) ||
+      max_blocks_of(fxade::k_ade_one<float>, ade_smem(true), nsm, &b) ||
+      max_blocks_of(fxade::k_ade_batch<double>, ade_smem(false), nsm, &c) ||
+      max_blocks_of(fxade::k_ade_batch<float>, ade_smem(true), nsm, &e))
+    return -1;
+  *out = std::min(std::min(a, b), std::min(c, e));
   return 0;
 }

@@ -14,16 +14,6 @@
 #include "fx_common.cuh"
 #include "fx_internal.h"
 
-void fx_launch_finalize(const fx_dev& d, cudaStream_t s);
-void fx_launch_batch_begin(const fx_dev& d, cudaStream_t s);
-void fx_launch_mark_static(const fx_dev& d, cudaStream_t s);
-void fx_launch_hydro(const fx_dev& d, cudaStream_t s);
-void fx_launch_courant_scan(const fx_dev& d, cudaStream_t s);
-void fx_launch_ade(const fx_dev& d, int nstrips, int nblocks, cudaStream_t s);
-int fx_ade_rows_per_strip();
-int fx_ade_threads_per_block();
-int fx_ade_max_blocks(int* out);
-
 static thread_local std::string g_last_error;
 
 static const unsigned long long kInfBits = 0x7ff0000000000000ull;
@@ -47,33 +37,50 @@ int fx_fail(fx_ctx* ctx, int code, const char* fmt, ...) {
                      "%s failed: %s", #call, cudaGetErrorString(e_));                      \
   } while (0)
 
-// Fields with one plane per slot (the state after step n lives in plane
-// n % nslot); the others have a single plane.
-static bool slot_field(const char* name) {
-  return !strcmp(name, "h") || !strcmp(name, "h0") || !strcmp(name, "fe_1") || !strcmp(name, "fn_1");
+// A state field on the device: its planes (one per slot for the fields the
+// ADE sweep reads after later steps, see fx_common.cuh), its element type.
+struct FieldRef {
+  void* ptr = nullptr;
+  bool f32 = false;   // float (FP32 state) instead of double
+  bool slot = false;  // one plane per slot
+  bool pair = false;  // two planes, the current one is fx_pp(steps)
+};
+
+static FieldRef field_ref(fx_ctx* c, const char* name) {
+  fx_dev& d = c->d;
+  FieldRef r;
+  const bool p32 = d.prec32 != 0;
+  auto pick = [&](void* p64, void* p32v, bool slot, bool pair = false) {
+    r.ptr = p32 ? p32v : p64;
+    r.f32 = p32;
+    r.slot = slot;
+    r.pair = pair;
+  };
+  if (!strcmp(name, "zb")) r.ptr = d.zb;  // FP64 in both forms
+  else if (!strcmp(name, "z")) {
+    if (!p32) pick(d.z, nullptr, false, true);  // FP32: held as eta, see fx_upload / fx_download
+  } else if (!strcmp(name, "h")) pick(d.h, d.h_f, true);
+  else if (!strcmp(name, "qx")) pick(d.qx, d.qx_f, false, true);
+  else if (!strcmp(name, "qy")) pick(d.qy, d.qy_f, false, true);
+  else if (!strcmp(name, "twet")) pick(d.twet, d.twet_f, false);
+  else if (!strcmp(name, "h0")) pick(d.h0, d.h0_f, true);
+  else if (!strcmp(name, "fe_1")) pick(d.fe1, d.fe1_f, true);
+  else if (!strcmp(name, "fe_2")) pick(d.fe2, d.fe2_f, false);
+  else if (!strcmp(name, "fe_3")) pick(d.fe3, d.fe3_f, false);
+  else if (!strcmp(name, "fn_1")) pick(d.fn1, d.fn1_f, true);
+  else if (!strcmp(name, "fn_2")) pick(d.fn2, d.fn2_f, false);
+  else if (!strcmp(name, "fn_3")) pick(d.fn3, d.fn3_f, false);
+  else if (!strncmp(name, "conc", 4)) {
+    int k = name[4] ? atoi(name + 4) : 0;
+    if (k >= 0 && k < d.nchem)
+      pick(d.conc ? d.conc + (long long)k * d.plane : nullptr,
+           d.conc_f ? d.conc_f + (long long)k * d.plane : nullptr, false);
+  }
+  return r;
 }
 
-static double* field_ptr(fx_ctx* c, const char* name) {
-  fx_dev& d = c->d;
-  if (!strcmp(name, "z")) return d.z;
-  if (!strcmp(name, "zb")) return d.zb;
-  if (!strcmp(name, "h")) return d.h;
-  if (!strcmp(name, "qx")) return d.qx;
-  if (!strcmp(name, "qy")) return d.qy;
-  if (!strcmp(name, "twet")) return d.twet;
-  if (!strcmp(name, "h0")) return d.h0;
-  if (!strcmp(name, "fe_1")) return d.fe1;
-  if (!strcmp(name, "fe_2")) return d.fe2;
-  if (!strcmp(name, "fe_3")) return d.fe3;
-  if (!strcmp(name, "fn_1")) return d.fn1;
-  if (!strcmp(name, "fn_2")) return d.fn2;
-  if (!strcmp(name, "fn_3")) return d.fn3;
-  if (!strncmp(name, "conc", 4)) {
-    int k = name[4] ? atoi(name + 4) : 0;
-    if (k < 0 || k >= d.nchem) return nullptr;
-    return d.conc + (long long)k * d.plane;
-  }
-  return nullptr;
+static bool known_field(fx_ctx* c, const char* name) {
+  return !strcmp(name, "z") || field_ref(c, name).ptr != nullptr;
 }
 
 static int dev_alloc(fx_ctx* c, void** p, size_t bytes) {
@@ -95,7 +102,7 @@ static int read_ctl(fx_ctx* c) {
   return FX_OK;
 }
 
-static void fill_status(const fx_ctl& k, fx_status* st) {
+void fx_fill_status(const fx_ctl& k, fx_status* st) {
   if (!st) return;
   st->tim = k.tim;
   st->dtfl = k.dtfl;
@@ -107,6 +114,33 @@ static void fill_status(const fx_ctl& k, fx_status* st) {
   st->finished = k.finished;
   st->device_error = k.error;
   st->forcing_overrun = k.forcing_overrun;
+  st->budget_melt = k.budget_melt;
+  st->budget_out = k.budget_out;
+}
+
+// Copies the host descriptor of the domain to its device copy when it changed.
+int fx_sync_dev(fx_ctx* c) {
+  if (!c->dev_dirty) return FX_OK;
+  FX_CK(c, cudaMemcpyAsync(c->d_dev, &c->d, sizeof(fx_dev), cudaMemcpyHostToDevice, c->stream));
+  FX_CK(c, cudaStreamSynchronize(c->stream));
+  c->dev_dirty = false;
+  return FX_OK;
+}
+
+// Hydrodynamic tiles of 32 x r threads: the tile table and the descriptor.
+static int set_tile_rows(fx_ctx* c, int r) {
+  if (!fx_tile_rows_ok(r)) return fx_fail(c, FX_ERR_ARG, "tile_rows must be 4, 8 or 16 (got %d)", r);
+  std::vector<fx_tile> tiles;
+  fx_tiles_of(0, c->d.nr, c->d.nc, r, tiles);
+  FX_CK(c, cudaMemcpyAsync(c->d_tiles, tiles.data(), sizeof(fx_tile) * tiles.size(), cudaMemcpyHostToDevice,
+                           c->stream));
+  FX_CK(c, cudaStreamSynchronize(c->stream));
+  c->ntiles = (int)tiles.size();
+  c->d.tile_rows = r;
+  c->graph_dirty = true;
+  c->dev_dirty = true;
+  c->dev_version++;
+  return FX_OK;
 }
 
 extern "C" {
@@ -159,15 +193,39 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
     d.nslot = k + 1;  // a batch of k steps plus the state before it
     c->batch_steps = k;
   }
-  const size_t pb = (size_t)d.plane * sizeof(double);
   int rc = FX_OK;
-  double** fields[] = {&d.z, &d.zb, &d.qx, &d.qy, &d.twet, &d.fe2, &d.fe3, &d.fn2, &d.fn3};
-  double** slot_fields[] = {&d.h, &d.h0, &d.hpm, &d.fe1, &d.fn1};
-  for (double** f : fields)
-    if ((rc = dev_alloc(c, (void**)f, pb)) != FX_OK) goto fail;
-  for (double** f : slot_fields)
-    if ((rc = dev_alloc(c, (void**)f, pb * d.nslot)) != FX_OK) goto fail;
-  if ((rc = dev_alloc(c, (void**)&d.conc, pb * g->nchem)) != FX_OK) goto fail;
+  if (p->precision != 0 && p->precision != 1) {
+    rc = fx_fail(c, FX_ERR_ARG, "fx_create: precision must be 0 (FP64) or 1 (FP32)");
+    goto fail;
+  }
+  d.prec32 = p->precision;
+  if (!d.prec32) {
+    const size_t pb = (size_t)d.plane * sizeof(double);
+    double** fields[] = {&d.zb, &d.twet, &d.fe2, &d.fe3, &d.fn2, &d.fn3};
+    double** pair_fields[] = {&d.z, &d.qx, &d.qy};
+    double** slot_fields[] = {&d.h, &d.h0, &d.hpm, &d.fe1, &d.fn1};
+    for (double** f : fields)
+      if ((rc = dev_alloc(c, (void**)f, pb)) != FX_OK) goto fail;
+    for (double** f : pair_fields)
+      if ((rc = dev_alloc(c, (void**)f, 2 * pb)) != FX_OK) goto fail;
+    for (double** f : slot_fields)
+      if ((rc = dev_alloc(c, (void**)f, pb * d.nslot)) != FX_OK) goto fail;
+    if ((rc = dev_alloc(c, (void**)&d.conc, pb * g->nchem)) != FX_OK) goto fail;
+  } else {
+    const size_t pf = (size_t)d.plane * sizeof(float);
+    float** fields[] = {&d.sx, &d.sy, &d.twet_f, &d.fe2_f, &d.fe3_f, &d.fn2_f, &d.fn3_f};
+    float** pair_fields[] = {&d.eta, &d.qx_f, &d.qy_f};
+    float** slot_fields[] = {&d.h_f, &d.h0_f, &d.hpm_f, &d.fe1_f, &d.fn1_f};
+    if ((rc = dev_alloc(c, (void**)&d.zb, (size_t)d.plane * sizeof(double))) != FX_OK) goto fail;
+    for (float** f : fields)
+      if ((rc = dev_alloc(c, (void**)f, pf)) != FX_OK) goto fail;
+    for (float** f : pair_fields)
+      if ((rc = dev_alloc(c, (void**)f, 2 * pf)) != FX_OK) goto fail;
+    for (float** f : slot_fields)
+      if ((rc = dev_alloc(c, (void**)f, pf * d.nslot)) != FX_OK) goto fail;
+    if ((rc = dev_alloc(c, (void**)&d.conc_f, pf * g->nchem)) != FX_OK) goto fail;
+  }
+  if ((rc = dev_alloc(c, (void**)&c->d_mass, sizeof(double) * (1 + FX_MAX_CHEM))) != FX_OK) goto fail;
   if ((rc = dev_alloc(c, (void**)&d.flags, (size_t)d.plane * d.nslot)) != FX_OK) goto fail;
   if ((rc = dev_alloc(c, (void**)&d.ctl, sizeof(fx_ctl))) != FX_OK) goto fail;
   {
@@ -195,6 +253,16 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
     int want = (units + per_block - 1) / per_block;
     c->ade_blocks = want < maxb ? want : maxb;
   }
+  {
+    // this domain's tile table (domain 0 of a batch of one), sized for the
+    // smallest tiles (most entries)
+    std::vector<fx_tile> tiles;
+    fx_tiles_of(0, g->nrows, g->ncols, 4, tiles);
+    c->nunits = c->batch_steps * g->nchem * c->ade_strips;
+    if ((rc = dev_alloc(c, (void**)&c->d_tiles, sizeof(fx_tile) * tiles.size())) != FX_OK) goto fail;
+    if ((rc = dev_alloc(c, (void**)&c->d_dev, sizeof(fx_dev))) != FX_OK) goto fail;
+    if ((rc = set_tile_rows(c, 8)) != FX_OK) goto fail;
+  }
   e = cudaMallocHost((void**)&c->ctl_host, sizeof(fx_ctl));
   if (e != cudaSuccess) {
     rc = fx_fail(c, FX_ERR_CUDA, "cudaMallocHost failed: %s", cudaGetErrorString(e));
@@ -214,6 +282,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
     goto fail;
   }
   c->h_min_print = p->h_min_print;
+  if ((rc = fx_sync_dev(c)) != FX_OK) goto fail;
   *out = c;
   return FX_OK;
 fail:
@@ -238,35 +307,120 @@ int fx_device_bytes(const fx_ctx* c, long long* bytes) {
   return FX_OK;
 }
 
+int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long long* bytes) {
+  if (!g || !p || !bytes || g->nrows < 2 || g->ncols < 2 || g->nchem < 1 || g->nchem > FX_MAX_CHEM)
+    return fx_fail(nullptr, FX_ERR_ARG, "fx_footprint: bad argument");
+  // the allocations of fx_create, field by field, plus the extension grids
+  const long long ld = ((g->nrows + 2 + FX_ROFF + 31) / 32) * 32;
+  const long long plane = ld * (g->ncols + 2);
+  long long k = p->steps_in_flight > 0 ? p->steps_in_flight : 8;
+  if (k > FX_MAX_SLOTS - 1) k = FX_MAX_SLOTS - 1;
+  const long long nslot = k + 1;
+  const long long strips = (g->nrows + fx_ade_rows_per_strip() - 1) / fx_ade_rows_per_strip();
+  const long long gx = (g->nrows + 30) / 31, gy = (g->ncols + 6) / 7;
+  long long b = 0;
+  if (p->precision == 1)
+    b += plane * (8 + 7 * 4 + 3 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids);
+  else
+    b += plane * (6 * 8 + 3 * 2 * 8 + 5 * 8 * nslot + 8LL * g->nchem + 8LL * extension_grids);
+  b += plane * nslot;                                   // flags
+  b += (long long)sizeof(fx_ctl) + 3 * FX_METEO_ROWS * 4 + (long long)sizeof(fx_dev);
+  b += 8LL * nslot * g->nchem * strips * (g->ncols + 2) * 3 + 8LL * nslot * g->nchem * strips;
+  b += (long long)sizeof(fx_tile) * gx * gy + (long long)sizeof(fx_unit) * k * g->nchem * strips;
+  b += 8LL * (1 + FX_MAX_CHEM);
+  *bytes = b;
+  return FX_OK;
+}
+
+// Copies a host grid (double, GlobVar layout) into `planes` consecutive
+// planes of a device field, converting to float for FP32 fields.
+static int put_grid(fx_ctx* c, void* dst, bool f32, int planes, const double* host) {
+  const int mr = c->d.nr + 2, mc = c->d.nc + 2;
+  const size_t esz = f32 ? sizeof(float) : sizeof(double);
+  std::vector<float> tmp;
+  const void* src = host;
+  if (f32) {
+    tmp.resize((size_t)mr * mc);
+    for (size_t i = 0; i < tmp.size(); ++i) tmp[i] = (float)host[i];
+    src = tmp.data();
+  }
+  for (int k = 0; k < planes; ++k)
+    FX_CK(c, cudaMemcpy2DAsync((char*)dst + (k * c->d.plane + FX_ROFF) * esz, (size_t)c->d.ld * esz, src,
+                               (size_t)mr * esz, (size_t)mr * esz, (size_t)mc, cudaMemcpyHostToDevice, c->stream));
+  FX_CK(c, cudaStreamSynchronize(c->stream));
+  return FX_OK;
+}
+
+// Copies one plane of a device field into a host grid (double).
+static int get_grid(fx_ctx* c, const void* src, bool f32, double* host) {
+  const int mr = c->d.nr + 2, mc = c->d.nc + 2;
+  const size_t esz = f32 ? sizeof(float) : sizeof(double);
+  std::vector<float> tmp;
+  void* dst = host;
+  if (f32) {
+    tmp.resize((size_t)mr * mc);
+    dst = tmp.data();
+  }
+  FX_CK(c, cudaMemcpy2DAsync(dst, (size_t)mr * esz, (const char*)src + FX_ROFF * esz, (size_t)c->d.ld * esz,
+                             (size_t)mr * esz, (size_t)mc, cudaMemcpyDeviceToHost, c->stream));
+  FX_CK(c, cudaStreamSynchronize(c->stream));
+  if (f32)
+    for (size_t i = 0; i < tmp.size(); ++i) host[i] = (double)tmp[i];
+  return FX_OK;
+}
+
+// FP32 state: z = zb + eta on the host (or the z still waiting for fx_prepare).
+static int get_z32(fx_ctx* c, double* host) {
+  const size_t n = (size_t)(c->d.nr + 2) * (c->d.nc + 2);
+  if (!c->z_pending.empty()) {
+    std::copy(c->z_pending.begin(), c->z_pending.end(), host);
+    return FX_OK;
+  }
+  std::vector<double> eta(n);
+  int rc = read_ctl(c);
+  if (!rc) rc = get_grid(c, c->d.zb, false, host);
+  if (!rc) rc = get_grid(c, c->d.eta + fx_pp(c->d, c->ctl_host->steps), true, eta.data());
+  if (rc) return rc;
+  for (size_t i = 0; i < n; ++i) host[i] += eta[i];
+  return FX_OK;
+}
+
 int fx_upload(fx_ctx* c, const char* field, const double* host) {
   if (!c || !field || !host) return fx_fail(c, FX_ERR_ARG, "fx_upload: null argument");
-  double* dst = field_ptr(c, field);
-  if (!dst) return fx_fail(c, FX_ERR_ARG, "fx_upload: unknown field '%s'", field);
-  const int mr = c->d.nr + 2, mc = c->d.nc + 2;
-  const int planes = slot_field(field) ? c->d.nslot : 1;  // every slot holds the uploaded state
-  for (int k = 0; k < planes; ++k)
-    FX_CK(c, cudaMemcpy2DAsync(dst + k * c->d.plane + FX_ROFF, (size_t)c->d.ld * sizeof(double), host,
-                               (size_t)mr * sizeof(double), (size_t)mr * sizeof(double), (size_t)mc,
-                               cudaMemcpyHostToDevice, c->stream));
-  FX_CK(c, cudaStreamSynchronize(c->stream));
+  if (!known_field(c, field)) return fx_fail(c, FX_ERR_ARG, "fx_upload: unknown field '%s'", field);
+  const size_t n = (size_t)(c->d.nr + 2) * (c->d.nc + 2);
+  int rc;
+  if (c->d.prec32 && !strcmp(field, "z")) {
+    c->z_pending.assign(host, host + n);  // converted by fx_prepare with the bed then current
+  } else if (c->d.prec32 && !strcmp(field, "zb")) {
+    // z stays what it was (as for FP64 state): keep it until fx_prepare
+    if (c->z_pending.empty()) {
+      c->z_pending.resize(n);
+      if ((rc = get_z32(c, c->z_pending.data()))) return rc;
+    }
+    if ((rc = put_grid(c, c->d.zb, false, 1, host))) return rc;
+  } else {
+    const FieldRef f = field_ref(c, field);
+    // every slot (and both planes of a pair) holds the uploaded state
+    if ((rc = put_grid(c, f.ptr, f.f32, f.slot ? c->d.nslot : (f.pair ? 2 : 1), host))) return rc;
+  }
   c->prepared = false;
   return FX_OK;
 }
 
 int fx_download(fx_ctx* c, const char* field, double* host) {
   if (!c || !field || !host) return fx_fail(c, FX_ERR_ARG, "fx_download: null argument");
-  double* src = field_ptr(c, field);
-  if (!src) return fx_fail(c, FX_ERR_ARG, "fx_download: unknown field '%s'", field);
-  if (slot_field(field)) {
+  if (!known_field(c, field)) return fx_fail(c, FX_ERR_ARG, "fx_download: unknown field '%s'", field);
+  if (c->d.prec32 && !strcmp(field, "z")) return get_z32(c, host);
+  const FieldRef f = field_ref(c, field);
+  const size_t esz = f.f32 ? sizeof(float) : sizeof(double);
+  const char* src = (const char*)f.ptr;
+  if (f.slot || f.pair) {
     int rc = read_ctl(c);
     if (rc) return rc;
-    src += fx_slot(c->d, c->ctl_host->steps);
+    src += (f.slot ? fx_slot(c->d, c->ctl_host->steps) : fx_pp(c->d, c->ctl_host->steps)) * esz;
   }
-  const int mr = c->d.nr + 2, mc = c->d.nc + 2;
-  FX_CK(c, cudaMemcpy2DAsync(host, (size_t)mr * sizeof(double), src + FX_ROFF, (size_t)c->d.ld * sizeof(double),
-                             (size_t)mr * sizeof(double), (size_t)mc, cudaMemcpyDeviceToHost, c->stream));
-  FX_CK(c, cudaStreamSynchronize(c->stream));
-  return FX_OK;
+  return get_grid(c, src, f.f32, host);
 }
 
 int fx_upload_flags(fx_ctx* c, const float* ldry, const float* wall) {
@@ -315,38 +469,42 @@ int fx_set_forcing(fx_ctx* c, const float* tab, int has_meteo) {
   }
   c->d.store_all_fluxes = (c->store_all_opt || c->negative_forcing) ? 1 : 0;
   c->graph_dirty = true;
+  c->dev_dirty = true;
+    c->dev_version++;
   return FX_OK;
 }
 
-static int set_optional_field(fx_ctx* c, const double* host, const double** slot, const char* what) {
+// A per-cell extension grid: FP64 copy for FP64 state, FP32 copy for FP32.
+static int set_optional_field(fx_ctx* c, const double* host, const double** slot64, const float** slot32) {
+  const bool f32 = c->d.prec32 != 0;
+  c->graph_dirty = true;
+  c->dev_dirty = true;
+  c->dev_version++;
   if (!host) {
-    *slot = nullptr;
-    c->graph_dirty = true;
+    *slot64 = nullptr;
+    *slot32 = nullptr;
     return FX_OK;
   }
-  double* p = const_cast<double*>(*slot);
+  void* p = f32 ? (void*)*slot32 : (void*)*slot64;
   if (!p) {
-    int rc = dev_alloc(c, (void**)&p, (size_t)c->d.plane * sizeof(double));
+    int rc = dev_alloc(c, &p, (size_t)c->d.plane * (f32 ? sizeof(float) : sizeof(double)));
     if (rc != FX_OK) return rc;
   }
-  const int mr = c->d.nr + 2, mc = c->d.nc + 2;
-  FX_CK(c, cudaMemcpy2DAsync(p + FX_ROFF, (size_t)c->d.ld * sizeof(double), host, (size_t)mr * sizeof(double),
-                             (size_t)mr * sizeof(double), (size_t)mc, cudaMemcpyHostToDevice, c->stream));
-  FX_CK(c, cudaStreamSynchronize(c->stream));
-  (void)what;
-  *slot = p;
-  c->graph_dirty = true;
+  int rc = put_grid(c, p, f32, 1, host);
+  if (rc) return rc;
+  if (f32) *slot32 = (const float*)p;
+  else *slot64 = (const double*)p;
   return FX_OK;
 }
 
 int fx_set_manning(fx_ctx* c, const double* n) {
   if (!c) return FX_ERR_ARG;
-  return set_optional_field(c, n, &c->d.manning, "manning");
+  return set_optional_field(c, n, &c->d.manning, &c->d.manning_f);
 }
 
 int fx_set_melt_field(fx_ctx* c, const double* m) {
   if (!c) return FX_ERR_ARG;
-  return set_optional_field(c, m, &c->d.melt_mult, "melt");
+  return set_optional_field(c, m, &c->d.melt_mult, &c->d.melt_mult_f);
 }
 
 int fx_set_option(fx_ctx* c, const char* name, long long v) {
@@ -355,8 +513,11 @@ int fx_set_option(fx_ctx* c, const char* name, long long v) {
     c->store_all_opt = v != 0;
     c->d.store_all_fluxes = (c->store_all_opt || c->negative_forcing) ? 1 : 0;
     c->graph_dirty = true;
+    c->dev_dirty = true;
+    c->dev_version++;
     return FX_OK;
   }
+  if (!strcmp(name, "tile_rows")) return set_tile_rows(c, (int)v);
   return fx_fail(c, FX_ERR_ARG, "fx_set_option: unknown option '%s'", name);
 }
 
@@ -367,8 +528,33 @@ int fx_prepare(fx_ctx* c) {
   c->ctl_host->acc_dtmin = kInfBits;
   c->ctl_host->acc_hmax = 0ull;
   FX_CK(c, cudaMemcpyAsync(c->d.ctl, c->ctl_host, sizeof(fx_ctl), cudaMemcpyHostToDevice, c->stream));
-  fx_launch_mark_static(c->d, c->stream);
-  fx_launch_courant_scan(c->d, c->stream);
+  if ((rc = fx_sync_dev(c))) return rc;
+  if (c->d.prec32) {
+    if (!c->z_pending.empty()) {
+      // stage z in the field layout and convert it with the current bed
+      double* z = nullptr;
+      FX_CK(c, cudaMalloc((void**)&z, (size_t)c->d.plane * sizeof(double)));
+      int r2 = FX_OK;
+      const int mr = c->d.nr + 2, mc = c->d.nc + 2;
+      cudaError_t e = cudaMemsetAsync(z, 0, (size_t)c->d.plane * sizeof(double), c->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(z + FX_ROFF, (size_t)c->d.ld * sizeof(double), c->z_pending.data(),
+                              (size_t)mr * sizeof(double), (size_t)mr * sizeof(double), (size_t)mc,
+                              cudaMemcpyHostToDevice, c->stream);
+      if (e == cudaSuccess) {
+        fx_launch_eta_from_z(c->d, z, c->stream);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) r2 = fx_fail(c, FX_ERR_CUDA, "FP32 depth conversion failed: %s", cudaGetErrorString(e));
+      cudaFree(z);
+      if (r2) return r2;
+      c->z_pending.clear();
+    }
+    fx_launch_bed_slopes(c->d, c->stream);
+  }
+  fx_launch_mark_static(c->d_dev, 0, c->stream);
+  fx_launch_courant_scan(c->d_dev, c->d_tiles, c->ntiles, c->d.tile_rows, c->stream);
   FX_CK(c, cudaGetLastError());
   FX_CK(c, cudaStreamSynchronize(c->stream));
   c->prepared = true;
@@ -380,15 +566,17 @@ int fx_prepare(fx_ctx* c) {
 // One batch of m steps: the clock and the hydrodynamics step by step, then
 // the ADE sweeps of all m steps in one launch (fx_ade.cu).
 static void launch_batch(fx_ctx* c, int m) {
-  fx_launch_batch_begin(c->d, c->stream);
+  fx_launch_batch_begin(c->d_dev, 1, c->stream);
   for (int i = 0; i < m; ++i) {
-    fx_launch_finalize(c->d, c->stream);
-    fx_launch_hydro(c->d, c->stream);
+    fx_launch_finalize(c->d_dev, 1, c->stream);
+    fx_launch_hydro_one(c->d, c->stream);
   }
-  fx_launch_ade(c->d, c->ade_strips, c->ade_blocks, c->stream);
+  fx_launch_ade_one(c->d, c->nunits, c->ade_blocks, c->stream);
 }
 
 static int ensure_graph(fx_ctx* c) {
+  int rc = fx_sync_dev(c);
+  if (rc) return rc;
   if (c->graph_exec && !c->graph_dirty) return FX_OK;
   if (c->graph_exec) {
     cudaGraphExecDestroy(c->graph_exec);
@@ -439,7 +627,7 @@ int fx_step(fx_ctx* c, int nsteps, fx_status* st) {
   if (left > 0) launch_batch(c, left);
   FX_CK(c, cudaGetLastError());
   if ((rc = read_ctl(c))) return rc;
-  fill_status(*c->ctl_host, st);
+  fx_fill_status(*c->ctl_host, st);
   return status_rc(c);
 }
 
@@ -458,7 +646,7 @@ int fx_run_to_print(fx_ctx* c, fx_status* st) {
     rc = fx_step(c, (int)n, nullptr);
     if (rc) return rc;
   }
-  fill_status(*c->ctl_host, st);
+  fx_fill_status(*c->ctl_host, st);
   return status_rc(c);
 }
 
@@ -477,11 +665,29 @@ int fx_get_status(fx_ctx* c, fx_status* st) {
   if (!c || !st) return FX_ERR_ARG;
   int rc = read_ctl(c);
   if (rc) return rc;
-  fill_status(*c->ctl_host, st);
+  fx_fill_status(*c->ctl_host, st);
   return FX_OK;
 }
 
 void* fx_stream(fx_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int fx_mass(fx_ctx* c, double* water, double* solute_mass) {
+  if (!c || !water) return fx_fail(c, FX_ERR_ARG, "fx_mass: null argument");
+  if (!c->prepared) {
+    int rc = fx_prepare(c);
+    if (rc) return rc;
+  }
+  double out[1 + FX_MAX_CHEM];
+  FX_CK(c, cudaMemsetAsync(c->d_mass, 0, sizeof(out), c->stream));
+  fx_launch_mass(c->d, c->d_mass, c->stream);
+  FX_CK(c, cudaGetLastError());
+  FX_CK(c, cudaMemcpyAsync(out, c->d_mass, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+  FX_CK(c, cudaStreamSynchronize(c->stream));
+  *water = out[0];
+  if (solute_mass)
+    for (int k = 0; k < c->d.nchem; ++k) solute_mass[k] = out[1 + k];
+  return FX_OK;
+}
 
 int fx_time_steps(fx_ctx* c, int n, double* ms_total, double* ms_hydro, double* ms_ade) {
   if (!c || n < 1) return FX_ERR_ARG;
@@ -489,7 +695,9 @@ int fx_time_steps(fx_ctx* c, int n, double* ms_total, double* ms_hydro, double* 
     int rc = fx_prepare(c);
     if (rc) return rc;
   }
-  int rc = read_ctl(c);
+  int rc = fx_sync_dev(c);
+  if (rc) return rc;
+  rc = read_ctl(c);
   if (rc) return rc;
   if ((rc = set_stop(c, c->ctl_host->steps + n))) return rc;
   // events: the start, then per step: after its clock update and after its
@@ -511,17 +719,17 @@ int fx_time_steps(fx_ctx* c, int n, double* ms_total, double* ms_hydro, double* 
   for (int left = n; left > 0 && !erc;) {
     const int m = left < K ? left : K;
     left -= m;
-    fx_launch_batch_begin(c->d, c->stream);
+    fx_launch_batch_begin(c->d_dev, 1, c->stream);
     for (int i = 0; i < m && !erc; ++i) {
-      fx_launch_finalize(c->d, c->stream);
+      fx_launch_finalize(c->d_dev, 1, c->stream);
       if ((erc = record(&a))) break;
-      fx_launch_hydro(c->d, c->stream);
+      fx_launch_hydro_one(c->d, c->stream);
       if ((erc = record(&b))) break;
       hyd.push_back({a, b});
     }
     if (erc) break;
     a = b;
-    fx_launch_ade(c->d, c->ade_strips, c->ade_blocks, c->stream);
+    fx_launch_ade_one(c->d, c->nunits, c->ade_blocks, c->stream);
     if ((erc = record(&b))) break;
     ade.push_back({a, b});
   }
@@ -548,6 +756,36 @@ int fx_time_steps(fx_ctx* c, int n, double* ms_total, double* ms_hydro, double* 
   if (ms_ade) *ms_ade = ta;
   if ((rc = read_ctl(c))) return rc;
   return status_rc(c);
+}
+
+int fx_autotune(fx_ctx* c, int trial_steps, int* tile_rows) {
+  if (!c || trial_steps < 1) return fx_fail(c, FX_ERR_ARG, "fx_autotune: bad argument");
+  // Each candidate runs trial_steps real steps (results do not depend on the
+  // tile shape); the hydrodynamic kernel time per step decides.
+  const int cand[3] = {4, 8, 16};
+  double best_ms = 0.0;
+  int best = c->d.tile_rows;
+  for (int r : cand) {
+    int rc = set_tile_rows(c, r);
+    if (rc) return rc;
+    rc = read_ctl(c);
+    if (rc) return rc;
+    const long long s0 = c->ctl_host->steps;
+    double tot = 0, hyd = 0, ade = 0;
+    rc = fx_time_steps(c, trial_steps, &tot, &hyd, &ade);
+    if (rc) return rc;
+    const long long ran = c->ctl_host->steps - s0;
+    if (ran < 1) continue;  // the run stopped (output due or over): nothing measured
+    const double ms = hyd / (double)ran;
+    if (best_ms == 0.0 || ms < best_ms) {
+      best_ms = ms;
+      best = r;
+    }
+  }
+  int rc = set_tile_rows(c, best);
+  if (rc) return rc;
+  if (tile_rows) *tile_rows = best;
+  return FX_OK;
 }
 
 }  // extern "C"

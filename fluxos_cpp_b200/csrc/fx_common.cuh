@@ -67,6 +67,11 @@ struct fx_ctl {
   int error;             // FX_DEVERR_* set by a kernel
   int pad_;
   long long batch;       // counts launch batches; the ADE sweep takes this batch's steps
+  // water budget since the last reset, FP64 [m^3]: melt added to the cells,
+  // and water that left through the outflow faces (E face of irow = NROWS,
+  // N face of icol = NCOLS)
+  double budget_melt;
+  double budget_out;
   fx_steprec rec[FX_MAX_SLOTS];  // per-slot record of the last steps
 };
 
@@ -90,11 +95,13 @@ struct fx_dev {
   int volrat_mode;    // 0: edge flux = weir formula, 1: edge flux = 0
   int ade;            // ADE module on
   int store_all_fluxes;  // 1 when forcing can remove water (see k_hydro)
-  int pad_;
+  int tile_rows;         // hydrodynamic tile: 32 x tile_rows threads (4, 8 or 16)
   double dcoef[FX_MAX_CHEM];
   // state. h, h0, fe1, fn1 and flags hold `nslot` planes each: the state
   // after step n lives in plane n % nslot, so the ADE sweep of a step can run
-  // after the hydrodynamics of the following steps (fx_ade.cu).
+  // after the hydrodynamics of the following steps (fx_ade.cu). z, qx, qy
+  // (eta, qx_f, qy_f) hold two planes: the state after step n is in plane
+  // n & 1 (fx_pp).
   int nslot;
   int pad3_;
   double *z, *zb, *h, *qx, *qy, *twet, *h0;
@@ -112,10 +119,33 @@ struct fx_dev {
   int has_meteo;
   int pad2_;
   fx_ctl* ctl;
+  // Single-precision state (prec32 = 1, fx_hydro.cu hydro_tile32): the depth
+  // above the bed eta = z - zb is stored, and the bed enters only through
+  // its differences to the east and north neighbours (sx = zb(E) - zb(P),
+  // sy = zb(N) - zb(P)), so water-surface differences are sx + (eta_E -
+  // eta_P) and thin films keep their digits. zb stays FP64 for output.
+  int prec32;
+  int pad4_;
+  float *eta, *sx, *sy, *qx_f, *qy_f, *twet_f;
+  float *h_f, *h0_f, *hpm_f, *fe1_f, *fn1_f;  // nslot planes each
+  float *fe2_f, *fe3_f, *fn2_f, *fn3_f;
+  float* conc_f;                              // nchem planes
+  const float* manning_f;
+  const float* melt_mult_f;
   // ADE sweep scratch
   double* ade_bnd;                 // per slot, solute, strip: (ncols+2) x 3
   unsigned long long* ade_prog;    // per slot, solute, strip: step<<32 | warp steps done
   long long plane;                 // elements per field = ld * (nc + 2)
+};
+
+// Work tables of a batch of domains (one domain is a batch of one).
+// A hydrodynamic tile: block (bx, by) of domain dom.
+struct fx_tile {
+  int dom, bx, by, pad;
+};
+// An ADE unit: strip s of solute k at the jj-th step of the batch, domain dom.
+struct fx_unit {
+  int dom, jj, k, s;
 };
 
 // x / dxy and x / dxy^2. When dxy is a power of two the quotient is an
@@ -144,4 +174,11 @@ __host__ __device__ inline long long fx_ix(const fx_dev& d, int irow, int icol) 
 // Offset of the slot plane that holds the state after step n.
 __host__ __device__ inline long long fx_slot(const fx_dev& d, long long step) {
   return (step % d.nslot) * d.plane;
+}
+
+// Offset of the plane of z (eta), qx, qy that holds the state after step n:
+// these fields have two planes, so a step reads one while it writes the
+// other (a tile reads its neighbours' cells as they were before the step).
+__host__ __device__ inline long long fx_pp(const fx_dev& d, long long step) {
+  return (step & 1) * d.plane;
 }

@@ -20,34 +20,46 @@
 // reference bit for bit except where noted at fx_pow15.
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "fx_common.cuh"
 
 namespace fx {
 
-// A block of 32 x 8 threads owns a tile of 31 rows (irow) x 7 columns (icol):
-// with its west row and south column of halo faces the tile has exactly
-// 32 x 8 = 256 face-flux cells, one per thread, so the flux phase runs in a
-// single wave and no warp waits at the barrier for a second round.
-constexpr int BX = 32, BY = 8;                  // threads
-constexpr int TX = 31, TY = 7;                  // owned cells
-constexpr int SX = TX + 3, SY = TY + 3;        // stencil: rows irow0-2..irow0+TX, cols icol0-2..icol0+TY
-constexpr int FXN = TX + 1, FYN = TY + 1;      // fluxes: rows irow0-1..irow0+TX-1, cols icol0-1..icol0+TY-1
-constexpr int NSTEN = SX * SY, NFLUX = FXN * FYN;
-constexpr int NTHREADS = BX * BY;
-static_assert(NFLUX == NTHREADS, "one face-flux cell per thread");
+// A block of 32 x BY threads owns a tile of 31 rows (irow) x BY-1 columns
+// (icol): with its west row and south column of halo faces the tile has
+// exactly 32 x BY face-flux cells, one per thread, so the flux phase runs in
+// a single wave and no warp waits at the barrier for a second round. BY (the
+// tile rows along icol: 4, 8 or 16) is chosen per domain or batch, by the
+// autotuner (fx_autotune) or fx_set_option("tile_rows").
+constexpr int BX = 32;          // threads along irow: one warp
+constexpr int TX = 31;          // owned rows
+constexpr int SX = TX + 3;      // stencil rows irow0-2..irow0+TX
+constexpr int FXN = TX + 1;     // flux rows irow0-1..irow0+TX-1
+template <int BY>
+struct Tile {
+  static constexpr int TY = BY - 1;            // owned columns
+  static constexpr int SY = TY + 3;            // stencil columns icol0-2..icol0+TY
+  static constexpr int FYN = TY + 1;           // flux columns icol0-1..icol0+TY-1
+  static constexpr int NSTEN = SX * SY, NFLUX = FXN * FYN, NTHREADS = BX * BY;
+  static_assert(NFLUX == NTHREADS, "one face-flux cell per thread");
+};
 
 // stencil cell classes
 constexpr unsigned char C_DRY = 1;   // Loop-1 ldry == 1 (interior cells only)
 constexpr unsigned char C_WALL = 2;  // innerNeumannBCWeir == 1
 constexpr unsigned char C_INT = 4;   // interior cell (1..NROWS, 1..NCOLS)
 
+template <int BY>
 struct HydroSmem {
+  static constexpr int NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX, NW = Tile<BY>::NTHREADS / 32;
+  double budget[2 * NW];
   double z[NSTEN], zb[NSTEN], qx[NSTEN], qy[NSTEN];
   double f[6][NFLUX];
   unsigned char cls[NSTEN];
   short wet_list[NFLUX], dry_list[NFLUX], stale_list[NFLUX];
   int nwet, ndry, nstale;
-  double red_dt[NTHREADS / 32], red_h[NTHREADS / 32];
+  double red_dt[NW], red_h[NW];
 };
 
 // sqrt(h)^3 = pow(h, 1.5) for h >= 0, correctly rounded: s = sqrt(h) is
@@ -87,7 +99,8 @@ __device__ __forceinline__ double fx_cbrt(double x) {
 __device__ __forceinline__ int sidx(int sr, int sc) { return sc * SX + sr; }
 
 // solver_wetdomain.cpp:27-342 for the flux cell at stencil (sr, sc).
-__device__ void solver_wet(const fx_dev& d, const HydroSmem& S, int sr, int sc, int irow, int icol,
+template <class SM>
+__device__ void solver_wet(const fx_dev& d, const SM& S, int sr, int sc, int irow, int icol,
                            double dtl, double out[6]) {
   const double hdryl = d.hdry, gaccl = d.gaccl;
   const int P = sidx(sr, sc), W = sidx(sr - 1, sc), E = sidx(sr + 1, sc);
@@ -310,7 +323,8 @@ __device__ void solver_wet(const fx_dev& d, const HydroSmem& S, int sr, int sc, 
 }
 
 // solver_drydomain.cpp:78-194 (the cell is dry and has a wet neighbour).
-__device__ void solver_dry(const fx_dev& d, const HydroSmem& S, int sr, int sc, int irow, int icol,
+template <class SM>
+__device__ void solver_dry(const fx_dev& d, const SM& S, int sr, int sc, int irow, int icol,
                            double dtl, double out[6]) {
   const int P = sidx(sr, sc), E = sidx(sr + 1, sc), N = sidx(sr, sc + 1);
   const double gaccl = d.gaccl;
@@ -394,7 +408,8 @@ __device__ __forceinline__ void courant_cell(const fx_dev& d, double h, double q
 }
 
 // Block-wide min/max followed by one atomic each on the control block.
-__device__ void reduce_courant(const fx_dev& d, HydroSmem& S, double dtc, double hm) {
+template <class SM>
+__device__ void reduce_courant(const fx_dev& d, SM& S, double dtc, double hm) {
   for (int o = 16; o > 0; o >>= 1) {
     dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
     hm = fmax(hm, __shfl_xor_sync(0xffffffffu, hm, o));
@@ -418,47 +433,537 @@ __device__ void reduce_courant(const fx_dev& d, HydroSmem& S, double dtc, double
   }
 }
 
-__device__ __forceinline__ double melt_depth(const fx_dev& d, const fx_ctl& c, long long gi) {
+// The fields of the control block a step kernel reads.
+struct StepCtl {
+  double dtfl, meteoi, meteo_rate, mconc;
+  long long steps;
+  int live, active;
+};
+
+// Block sum of the step's water budget terms, one double atomic each.
+__device__ void reduce_budget(const fx_dev& d, double* red, double melt, double out) {
+  for (int o = 16; o > 0; o >>= 1) {
+    melt += __shfl_xor_sync(0xffffffffu, melt, o);
+    out += __shfl_xor_sync(0xffffffffu, out, o);
+  }
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nw = (blockDim.x * blockDim.y) / 32;
+  __syncthreads();
+  if ((tid & 31) == 0) {
+    red[2 * (tid >> 5)] = melt;
+    red[2 * (tid >> 5) + 1] = out;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < nw; ++w) {
+      a += red[2 * w];
+      b += red[2 * w + 1];
+    }
+    if (a != 0.0) atomicAdd(&d.ctl->budget_melt, a);
+    if (b != 0.0) atomicAdd(&d.ctl->budget_out, b);
+  }
+}
+
+__device__ __forceinline__ double melt_depth(const fx_dev& d, const StepCtl& c, long long gi) {
   if (d.melt_mult) return (double)c.meteo_rate * d.melt_mult[gi] / (1000. * 3600. * 24.) * c.dtfl;
   return c.meteoi;
 }
 
-__global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
-  __shared__ HydroSmem S;
-  const fx_ctl c = *d.ctl;
-  if (!c.live) return;
+
+// ===================== single-precision step (prec32) =======================
+// The same step as k_hydro's FP64 body, on the depth eta = z - zb and the bed
+// differences sx, sy (fx_common.cuh): every water-surface difference of the
+// reference is rewritten without the bed elevation itself,
+//   ze - zp = sx(P) + (eta_E - eta_P),  zp - zbpe = eta_P - sx(P)/2,
+//   ze - zbpe = eta_E + sx(P)/2,        h = max(0, eta),
+// and likewise to the north with sy. Flux, update and friction arithmetic is
+// FP32; the wet/dry threshold tests compare in FP64, the Courant candidates
+// and the water budget are FP64.
+
+template <int BY>
+struct HydroSmem32 {
+  static constexpr int NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX, NW = Tile<BY>::NTHREADS / 32;
+  double budget[2 * NW];
+  double red_dt[NW], red_h[NW];
+  float eta[NSTEN], sx[NSTEN], sy[NSTEN], qx[NSTEN], qy[NSTEN];
+  float f[6][NFLUX];
+  unsigned char cls[NSTEN];
+  short wet_list[NFLUX], dry_list[NFLUX], stale_list[NFLUX];
+  int nwet, ndry, nstale;
+};
+
+__device__ __forceinline__ float div_dxy_f(const fx_dev& d, float x) {
+  return d.dxy_pow2 ? x * (float)d.inv_dxy : x / (float)d.dxy;
+}
+
+template <class SM>
+__device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int irow, int icol,
+                             float dtl, float out[6]) {
+  const double hdry = d.hdry;
+  const float hdryl = (float)d.hdry, gaccl = (float)d.gaccl;
+  const int P = sidx(sr, sc), W = sidx(sr - 1, sc), E = sidx(sr + 1, sc);
+  const int Sx = sidx(sr, sc - 1), N = sidx(sr, sc + 1);
+  const int ES = sidx(sr + 1, sc - 1), EN = sidx(sr + 1, sc + 1), WN = sidx(sr - 1, sc + 1);
+  auto ksat = [&](int k) { return (S.cls[k] & C_INT) ? (float)d.ks : 0.0f; };
+  auto hat = [&](int k) { return fmaxf(0.0f, S.eta[k]); };
+  const float kspl = ksat(P);
+  const float nueml = (float)d.nueml;
+  const float dx = (float)d.dxy, dy = dx;
+  bool lroe = true;
+  float volrat = d.volrat_mode == 0 ? __int_as_float(0x7f800000) : 0.0f;
+  const bool ldp_dry = S.cls[P] & C_DRY, lde_dry = S.cls[E] & C_DRY, ldn_dry = S.cls[N] & C_DRY;
+  const float etap = S.eta[P], sxp = S.sx[P], syp = S.sy[P];
+  float qp = S.qx[P], qe = S.qx[E], qn = S.qx[N];
+  float rw = S.qy[W], rp = S.qy[P], re = S.qy[E], rn = S.qy[N];
+  const float hp = fmaxf(0.0f, etap);
+  const float hp0 = fmaxf(fmaxf(hdryl, hp), kspl);
+  const float hw = fmaxf(0.0f, S.eta[W]);
+  float he = fmaxf(0.0f, S.eta[E]);
+  const float hs = fmaxf(0.0f, S.eta[Sx]);
+  float hn = fmaxf(0.0f, S.eta[N]);
+  float hme = .5f * (hp + he), qme = .5f * (qp + qe), rme = .5f * (rp + re);
+  float hmn = .5f * (hp + hn), qmn = .5f * (qp + qn), rmn = .5f * (rp + rn);
+  float dze = sxp + (S.eta[E] - etap);
+  const float dqe = qe - qp, dre = re - rp;
+  float dzn = syp + (S.eta[N] - etap);
+  const float drn = rn - rp, dqn = qn - qp;
+  if (lde_dry) {
+    hme = fmaxf(0.0f, etap - .5f * sxp);
+    he = qe = re = 0.0f;
+    if ((double)hme > hdry) {
+      if (dze >= 0.0f) {
+        qme = rme = 0.0f;
+      } else {
+        dze = fminf(fabsf(dze), hme);
+        qme = 0.296f * dze * sqrtf(gaccl * dze);
+        volrat = 0.5f * dx * hp / dtl;
+        qme = fminf(qme, volrat);
+        rme = 0.0f;
+      }
+    } else {
+      qme = rme = hme = 0.0f;
+    }
+    lroe = false;
+  }
+  if (ldn_dry) {
+    hmn = fmaxf(0.0f, etap - .5f * syp);
+    hn = qn = rn = 0.0f;
+    if ((double)hmn > hdry) {
+      if (dzn >= 0.0f) {
+        qmn = rmn = 0.0f;
+      } else {
+        dzn = fminf(fabsf(dzn), hmn);
+        rmn = 0.296f * dzn * sqrtf(gaccl * dzn);
+        qmn = 0.0f;
+        volrat = 0.5f * dy * hp / dtl;
+        rmn = fminf(rmn, volrat);
+      }
+    } else {
+      qmn = rmn = hmn = 0.0f;
+    }
+    lroe = false;
+  }
+  const float cme = sqrtf(gaccl * hme), cmn = sqrtf(gaccl * hmn);
+  const float ume = qme / fmaxf(hme, hdryl), vme = rme / fmaxf(hme, hdryl);
+  const float umn = qmn / fmaxf(hmn, hdryl), vmn = rmn / fmaxf(hmn, hdryl);
+  const float hne = nueml * sqrtf(hp * he);  // (cvdef*us*h + nuem), us = 0
+  const float hnn = nueml * sqrtf(hp * hn);
+  const float up = qp / hp0;
+  const float un = qn / fmaxf(fmaxf(hn, hdryl), ksat(N));
+  const float us0 = S.qx[Sx] / fmaxf(fmaxf(hs, hdryl), ksat(Sx));
+  const float use0 = S.qx[ES] / fmaxf(fmaxf(hat(ES), hdryl), ksat(ES));
+  const float une = S.qx[EN] / fmaxf(fmaxf(hat(EN), hdryl), ksat(EN));
+  const float vp = rp / hp0;
+  const float ve = re / fmaxf(fmaxf(he, hdryl), ksat(E));
+  const float vw = rw / fmaxf(fmaxf(hw, hdryl), ksat(W));
+  const float vwn = S.qy[WN] / fmaxf(fmaxf(hat(WN), hdryl), ksat(WN));
+  const float ven = S.qy[EN] / fmaxf(fmaxf(hat(EN), hdryl), ksat(EN));
+  const float txye = hne * (div_dxy_f(d, ve - vp) + div_dxy_f(d, .25f * (un + une - us0 - use0)));
+  const float txyn = hnn * (div_dxy_f(d, un - up) + div_dxy_f(d, .25f * (ve + ven - vw - vwn)));
+  const float fe1c = qme, fe2c = qme * ume, fe3c = qme * vme - txye;
+  const float fn1c = rmn, fn2c = rmn * umn - txyn, fn3c = rmn * vmn;
+  float fe1r = 0.f, fe2r = 0.f, fe3r = 0.f, fn1r = 0.f, fn2r = 0.f, fn3r = 0.f;
+  if (lroe) {
+    float cc;
+    if ((double)hme > hdry) {
+      float dzea = fabsf(dze);
+      if (dzea > 0.5f * hme) {
+        dzea = fminf(dzea, fabsf(he - hp));
+        dze = copysignf(dzea, dze);
+      }
+      cc = .25f / cme;
+    } else {
+      cc = 0.0f;
+    }
+    float c1 = ume, c2 = ume + cme, c3 = ume - cme;
+    float c1a = fabsf(c1), c2a = fabsf(c2), c3a = fabsf(c3);
+    fe1r = -((c2 * c3a - c2a * c3) * dze + (c2a - c3a) * dqe) * cc;
+    fe2r = -(c2 * c3 * (c3a - c2a) * dze + (c2a * c2 - c3a * c3) * dqe) * cc;
+    fe3r = -(vme * (c2 * c3a - 2.f * cme * c1a - c2a * c3) * dze + vme * (c2a - c3a) * dqe + 2.f * cme * c1a * dre) * cc;
+    if (!ldp_dry && (double)hmn > hdry) {
+      float dzna = fminf(fabsf(dzn), fabsf(hn - hp));
+      dzn = copysignf(dzna, dzn);
+      cc = .25f / cmn;
+    } else {
+      cc = 0.0f;
+    }
+    c1 = vmn;
+    c2 = vmn + cmn;
+    c3 = vmn - cmn;
+    c1a = fabsf(c1);
+    c2a = fabsf(c2);
+    c3a = fabsf(c3);
+    fn1r = -((c2 * c3a - c2a * c3) * dzn + (c2a - c3a) * drn) * cc;
+    fn2r = -(umn * (c2 * c3a - 2.f * cmn * c1a - c2a * c3) * dzn + 2.f * cmn * c1a * dqn + umn * (c2a - c3a) * drn) * cc;
+    fn3r = -(c2 * c3 * (c3a - c2a) * dzn + (c2a * c2 - c3a * c3) * drn) * cc;
+  }
+  float fe1 = fe1c + fe1r;
+  const float fe2 = fe2c + fe2r + .5f * gaccl * (hme * hme);
+  const float fe3 = fe3c + fe3r;
+  float fn1 = fn1c + fn1r;
+  const float fn2 = fn2c + fn2r;
+  const float fn3 = fn3c + fn3r + .5f * gaccl * (hmn * hmn);
+  const float weir = sqrtf(gaccl) * hp * sqrtf(hp);
+  if (icol == 1 || icol == d.nc) fn1 = fminf(volrat, weir);
+  if (irow == 1 || irow == d.nr) fe1 = fminf(volrat, weir);
+  volrat = (float)d.arbase * hp / dtl;
+  if (volrat > 0.0f) {
+    if (fe1 > 0.0f && fn1 > 0.0f) {
+      if (fe1 * dy + fn1 * dx > volrat) {
+        const float cf = fn1 * dx / (fe1 * dy + fn1 * dx);
+        fe1 = div_dxy_f(d, (1.f - cf) * volrat);
+        fn1 = div_dxy_f(d, cf * volrat);
+      }
+    } else if (fe1 > 0.0f) {
+      fe1 = div_dxy_f(d, fminf(fe1 * dy, volrat));
+    } else if (fn1 > 0.0f) {
+      fn1 = div_dxy_f(d, fminf(fn1 * dx, volrat));
+    }
+  } else {
+    fe1 = fn1 = 0.0f;
+  }
+  out[0] = fe1;
+  out[1] = fe2;
+  out[2] = fe3;
+  out[3] = fn1;
+  out[4] = fn2;
+  out[5] = fn3;
+}
+
+template <class SM>
+__device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int irow, int icol,
+                             float dtl, float out[6]) {
+  const int P = sidx(sr, sc), E = sidx(sr + 1, sc), N = sidx(sr, sc + 1);
+  const float gaccl = (float)d.gaccl;
+  float volrat = d.volrat_mode == 0 ? __int_as_float(0x7f800000) : 0.0f;
+  const bool lde_dry = S.cls[E] & C_DRY, ldn_dry = S.cls[N] & C_DRY;
+  const float etap = S.eta[P], etae = S.eta[E], etan = S.eta[N], sxp = S.sx[P], syp = S.sy[P];
+  const float he = fmaxf(0.0f, etae), hn = fmaxf(0.0f, etan);
+  float dze = sxp + (etae - etap), dzn = syp + (etan - etap);
+  float fe1 = 0.f, fe2 = 0.f, fe3 = 0.f, fn1 = 0.f, fn2 = 0.f, fn3 = 0.f;
+  if (!lde_dry) {
+    float hme = fmaxf(0.0f, etae + .5f * sxp);
+    if ((double)hme > d.hdry) {
+      if (dze <= 0.0f) {
+        fe2 = .5f * gaccl * hme * hme;
+      } else {
+        dze = fminf(fabsf(dze), hme);
+        float qme = 0.296f * dze * sqrtf(gaccl * dze);
+        hme = 0.444f * dze;
+        volrat = (float)d.dxy * he / dtl;
+        qme = -fminf(qme, volrat);
+        fe1 = qme;
+        fe2 = qme * (qme / hme) + .5f * gaccl * hme * hme;
+      }
+    }
+  }
+  if (!ldn_dry) {
+    float hmn = fmaxf(0.0f, etan + .5f * syp);
+    if ((double)hmn > d.hdry) {
+      if (dzn <= 0.0f) {
+        fn3 = .5f * gaccl * hmn * hmn;
+      } else {
+        dzn = fminf(fabsf(dzn), hmn);
+        float rmn = 0.296f * dzn * sqrtf(gaccl * dzn);
+        hmn = 0.444f * dzn;
+        volrat = (float)d.dxy * hn / dtl;
+        rmn = -fminf(rmn, volrat);
+        fn1 = rmn;
+        fn3 = rmn * (rmn / hmn) + .5f * gaccl * hmn * hmn;
+      }
+    }
+  }
+  // the dry cell's own depth is taken as 0 (solver_drydomain.cpp:85): the weir is 0
+  if (icol == 1 || icol == d.nc) fn1 = fminf(volrat, 0.0f);
+  if (irow == 1 || irow == d.nr) fe1 = fminf(volrat, 0.0f);
+  out[0] = fe1;
+  out[1] = fe2;
+  out[2] = fe3;
+  out[3] = fn1;
+  out[4] = fn2;
+  out[5] = fn3;
+}
+
+template <int BY>
+__device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
+                                             HydroSmem32<BY>& S) {
+  constexpr int TY = Tile<BY>::TY, NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX;
+  constexpr int NTHREADS = Tile<BY>::NTHREADS;
   const int lx = threadIdx.x, ly = threadIdx.y;
   const int tid = ly * BX + lx;
-  const int irow0 = 1 + blockIdx.x * TX, icol0 = 1 + blockIdx.y * TY;
+  const int irow0 = 1 + tile.bx * TX, icol0 = 1 + tile.by * TY;
+  const int irow = irow0 + lx, icol = icol0 + ly;
+  const bool own = lx < TX && ly < TY && irow <= d.nr && icol <= d.nc;
+  const float dtl = (float)c.dtfl;
+  const bool melt_on = d.has_meteo != 0;
+  const long long sprev = fx_slot(d, c.steps - 1), scur = fx_slot(d, c.steps);
+  const long long pprev = fx_pp(d, c.steps - 1), pcur = fx_pp(d, c.steps);
+  double dtc = __longlong_as_double(0x7ff0000000000000LL), hm = 0.0, bmelt = 0.0, bout = 0.0;
+
+  if (!c.active) {
+    if (own) {
+      const long long gi = fx_ix(d, irow, icol);
+      const float etapre = d.eta[pprev + gi];
+      float eta1 = etapre;
+      const uint8_t fl = d.flags[sprev + gi];
+      const float hpre = fmaxf(0.0f, etapre);
+      uint8_t ld = (double)hpre > d.hdry ? 0 : 1;
+      float h1 = hpre;
+      if (melt_on && !(fl & FX_F_NODATA)) {
+        const double mi = melt_depth(d, c, gi);
+        bmelt = mi * d.arbase;
+        if (d.ade) d.hpm_f[scur + gi] = hpre;
+        eta1 = etapre + (float)mi;
+        h1 = fmaxf(eta1, 0.0f);
+        if ((double)h1 <= d.hdry) ld = 0;
+      }
+      const float qx = d.qx_f[pprev + gi], qy = d.qy_f[pprev + gi];
+      d.eta[pcur + gi] = eta1;
+      d.qx_f[pcur + gi] = qx;
+      d.qy_f[pcur + gi] = qy;
+      d.h_f[scur + gi] = h1;
+      d.h0_f[scur + gi] = h1;
+      d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+      if (scur != sprev) {
+        d.fe1_f[scur + gi] = d.fe1_f[sprev + gi];
+        d.fn1_f[scur + gi] = d.fn1_f[sprev + gi];
+      }
+      courant_cell(d, (double)h1, (double)qx, (double)qy, dtc, hm);
+    }
+    reduce_courant(d, S, dtc, hm);
+    reduce_budget(d, S.budget, bmelt, 0.0);
+    return;
+  }
+
+  if (tid == 0) {
+    S.nwet = 0;
+    S.ndry = 0;
+    S.nstale = 0;
+  }
+  for (int k = tid; k < NSTEN; k += NTHREADS) {
+    const int sr = k % SX, scc = k / SX;
+    const int r = irow0 - 2 + sr, q = icol0 - 2 + scc;
+    float eta = 0.f, sx = 0.f, sy = 0.f, qx = 0.f, qy = 0.f;
+    unsigned char cl = 0;
+    if (r >= 0 && r <= d.nr + 1 && q >= 0 && q <= d.nc + 1) {
+      const long long gi = fx_ix(d, r, q);
+      eta = d.eta[pprev + gi];
+      sx = d.sx[gi];
+      sy = d.sy[gi];
+      qx = d.qx_f[pprev + gi];
+      qy = d.qy_f[pprev + gi];
+      if (r >= 1 && r <= d.nr && q >= 1 && q <= d.nc) {
+        cl = C_INT;
+        const uint8_t fl = d.flags[sprev + gi];
+        if (fl & FX_F_WALL) cl |= C_WALL;
+        if (melt_on && !(fl & FX_F_NODATA)) eta = eta + (float)melt_depth(d, c, gi);
+        if ((double)fmaxf(0.0f, eta) <= d.hdry) {
+          qx = 0.f;
+          qy = 0.f;
+          cl |= C_DRY;
+        }
+      }
+    }
+    S.eta[k] = eta;
+    S.sx[k] = sx;
+    S.sy[k] = sy;
+    S.qx[k] = qx;
+    S.qy[k] = qy;
+    S.cls[k] = cl;
+  }
+  __syncthreads();
+  for (int k = tid; k < NFLUX; k += NTHREADS) {
+    const int fr = k % FXN, fc = k / FXN;
+    const int sr = fr + 1, scc = fc + 1;
+    const unsigned char cl = S.cls[sidx(sr, scc)];
+    if (!(cl & C_INT) || (cl & C_WALL)) {
+      for (int j = 0; j < 6; ++j) S.f[j][k] = 0.0f;
+      continue;
+    }
+    if (cl & C_DRY) {
+      const bool alldry = (S.cls[sidx(sr - 1, scc)] & C_DRY) && (S.cls[sidx(sr + 1, scc)] & C_DRY) &&
+                          (S.cls[sidx(sr, scc - 1)] & C_DRY) && (S.cls[sidx(sr, scc + 1)] & C_DRY);
+      if (alldry) S.stale_list[atomicAdd(&S.nstale, 1)] = (short)k;
+      else S.dry_list[atomicAdd(&S.ndry, 1)] = (short)k;
+    } else {
+      S.wet_list[atomicAdd(&S.nwet, 1)] = (short)k;
+    }
+  }
+  __syncthreads();
+  {
+    float o[6];
+    for (int i = tid; i < S.nwet; i += NTHREADS) {
+      const int k = S.wet_list[i];
+      const int fr = k % FXN, fc = k / FXN;
+      solver_wet32(d, S, fr + 1, fc + 1, irow0 - 1 + fr, icol0 - 1 + fc, dtl, o);
+      for (int j = 0; j < 6; ++j) S.f[j][k] = o[j];
+    }
+    for (int i = tid; i < S.ndry; i += NTHREADS) {
+      const int k = S.dry_list[i];
+      const int fr = k % FXN, fc = k / FXN;
+      solver_dry32(d, S, fr + 1, fc + 1, irow0 - 1 + fr, icol0 - 1 + fc, dtl, o);
+      for (int j = 0; j < 6; ++j) S.f[j][k] = o[j];
+    }
+    for (int i = tid; i < S.nstale; i += NTHREADS) {
+      const int k = S.stale_list[i];
+      const int fr = k % FXN, fc = k / FXN;
+      const long long gi = fx_ix(d, irow0 - 1 + fr, icol0 - 1 + fc);
+      S.f[0][k] = d.fe1_f[sprev + gi];
+      S.f[1][k] = d.fe2_f[gi];
+      S.f[2][k] = d.fe3_f[gi];
+      S.f[3][k] = d.fn1_f[sprev + gi];
+      S.f[4][k] = d.fn2_f[gi];
+      S.f[5][k] = d.fn3_f[gi];
+    }
+  }
+  __syncthreads();
+  if (own) {
+    const long long gi = fx_ix(d, irow, icol);
+    const int sP = sidx(lx + 2, ly + 2);
+    const int fP = (ly + 1) * FXN + (lx + 1), fW = (ly + 1) * FXN + lx, fS = ly * FXN + (lx + 1);
+    const unsigned char cl = S.cls[sP];
+    const bool wall = cl & C_WALL;
+    const uint8_t fl = d.flags[sprev + gi];
+    const float eta1 = S.eta[sP];
+    const float etapre = d.eta[pprev + gi];
+    float h0v = fmaxf(0.0f, etapre);
+    if (melt_on && !(fl & FX_F_NODATA)) {
+      h0v = fmaxf(eta1, 0.0f);
+      if (d.ade) d.hpm_f[scur + gi] = fmaxf(etapre, 0.0f);
+      bmelt = melt_depth(d, c, gi) * d.arbase;
+    }
+    if (!(cl & C_DRY)) d.twet_f[gi] += (float)(c.dtfl / 3600);
+    float dh = 0.f, dqx = 0.f, dqy = 0.f, qxfP = 0.f, qyfP = 0.f;
+    if (!wall) {
+      dh = (div_dxy_f(d, S.f[0][fW] - S.f[0][fP]) + div_dxy_f(d, S.f[3][fS] - S.f[3][fP])) * dtl;
+      dqx = (div_dxy_f(d, S.f[1][fW] - S.f[1][fP]) + div_dxy_f(d, S.f[4][fS] - S.f[4][fP])) * dtl;
+      dqy = (div_dxy_f(d, S.f[2][fW] - S.f[2][fP]) + div_dxy_f(d, S.f[5][fS] - S.f[5][fP])) * dtl;
+      qxfP = S.f[0][fP] * dtl;
+      qyfP = S.f[3][fP] * dtl;
+      const unsigned char clE = S.cls[sidx(lx + 3, ly + 2)], clN = S.cls[sidx(lx + 2, ly + 3)];
+      if (irow == d.nr || (clE & C_WALL)) bout += (double)S.f[0][fP] * d.dxy * c.dtfl;
+      if (icol == d.nc || (clN & C_WALL)) bout += (double)S.f[3][fP] * d.dxy * c.dtfl;
+    }
+    const unsigned char clW = S.cls[sidx(lx + 1, ly + 2)], clS = S.cls[sidx(lx + 2, ly + 1)];
+    const float qxfW = ((clW & C_INT) && !(clW & C_WALL)) ? S.f[0][fW] * dtl : 0.0f;
+    const float qyfS = ((clS & C_INT) && !(clS & C_WALL)) ? S.f[3][fS] * dtl : 0.0f;
+    const float eta = eta1 + dh;
+    const float h = fmaxf(0.0f, eta);
+    float qx, qy;
+    uint8_t ld;
+    if ((double)h < d.hdry || wall) {
+      qx = qy = 0.0f;
+      ld = 1;
+    } else {
+      qx = S.qx[sP] + dqx;
+      qy = S.qy[sP] + dqy;
+      qx = .1f * qxfW + .8f * qx + .1f * qxfP;
+      qy = .1f * qyfS + .8f * qy + .1f * qyfP;
+      ld = 0;
+    }
+    if (d.manning_f && ld == 0 && !wall) {
+      const float n = d.manning_f[gi];
+      if (n != 0.0f) {
+        const float qm = sqrtf(qx * qx + qy * qy);
+        const float den = 1.0f + dtl * (float)d.gaccl * n * n * qm / (h * h * cbrtf(h));
+        qx = qx / den;
+        qy = qy / den;
+      }
+    }
+    d.eta[pcur + gi] = eta;
+    d.h_f[scur + gi] = h;
+    d.qx_f[pcur + gi] = qx;
+    d.qy_f[pcur + gi] = qy;
+    d.h0_f[scur + gi] = h0v;
+    d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+    if ((cl & C_INT) && !wall) {
+      const bool computed =
+          !(cl & C_DRY) || !((S.cls[sidx(lx + 1, ly + 2)] & C_DRY) && (S.cls[sidx(lx + 3, ly + 2)] & C_DRY) &&
+                             (S.cls[sidx(lx + 2, ly + 1)] & C_DRY) && (S.cls[sidx(lx + 2, ly + 3)] & C_DRY));
+      d.fe1_f[scur + gi] = S.f[0][fP];
+      d.fn1_f[scur + gi] = S.f[3][fP];
+      if (computed && (d.store_all_fluxes || !((double)h > d.hdry))) {
+        d.fe2_f[gi] = S.f[1][fP];
+        d.fe3_f[gi] = S.f[2][fP];
+        d.fn2_f[gi] = S.f[4][fP];
+        d.fn3_f[gi] = S.f[5][fP];
+      }
+    } else if (scur != sprev) {
+      d.fe1_f[scur + gi] = 0.0f;
+      d.fn1_f[scur + gi] = 0.0f;
+    }
+    courant_cell(d, (double)h, (double)qx, (double)qy, dtc, hm);
+  }
+  reduce_courant(d, S, dtc, hm);
+  reduce_budget(d, S.budget, bmelt, bout);
+}
+
+// The FP64 step of one tile (the reference's arithmetic, bit for bit).
+template <int BY>
+__device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
+                                             HydroSmem<BY>& S) {
+  constexpr int TY = Tile<BY>::TY, NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX;
+  constexpr int NTHREADS = Tile<BY>::NTHREADS;
+  const int lx = threadIdx.x, ly = threadIdx.y;
+  const int tid = ly * BX + lx;
+  const int irow0 = 1 + tile.bx * TX, icol0 = 1 + tile.by * TY;
   const int irow = irow0 + lx, icol = icol0 + ly;
   const bool own = lx < TX && ly < TY && irow <= d.nr && icol <= d.nc;
   const double dtl = c.dtfl;
   const bool melt_on = d.has_meteo != 0;
 
   // Slot planes: the state after the previous step, and the one this step
-  // writes (h, h0, fe_1, fn_1, flags; see fx_common.cuh).
+  // writes (h, h0, fe_1, fn_1, flags), and the two planes of z, qx, qy (see
+  // fx_common.cuh): every block reads the previous step's plane, halo
+  // included, and writes the other.
   const long long sprev = fx_slot(d, c.steps - 1), scur = fx_slot(d, c.steps);
+  const long long pprev = fx_pp(d, c.steps - 1), pcur = fx_pp(d, c.steps);
 
   if (!c.active) {
     // No wet cell: the step is the Courant scan plus add_meteo only
     // (main.cpp:300-370, the solver block at :385 is skipped). The solute
     // dilution of add_meteo is applied by the ADE sweep (fx_ade.cu).
-    double dtc = __longlong_as_double(0x7ff0000000000000LL), hm = 0.0;
+    double dtc = __longlong_as_double(0x7ff0000000000000LL), hm = 0.0, bmelt = 0.0;
     if (own) {
       const long long gi = fx_ix(d, irow, icol);
-      const double zb = d.zb[gi], zpre = d.z[gi];
+      const double zb = d.zb[gi], zpre = d.z[pprev + gi];
       const uint8_t fl = d.flags[sprev + gi];
       const double hpre = fmax(0.0, zpre - zb);
       uint8_t ld = hpre > d.hdry ? 0 : 1;  // Courant scan (:308-320)
       double z1 = zpre, h1 = hpre;
       if (melt_on && zb != d.nodata) {
         const double mi = melt_depth(d, c, gi);
+        bmelt = mi * d.arbase;
         if (d.ade) d.hpm[scur + gi] = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
         z1 = zpre + mi;
         h1 = fmax(z1 - zb, 0.0);
         if (h1 <= d.hdry) ld = 0;  // common.cpp:219-222
-        d.z[gi] = z1;
       }
+      const double qx = d.qx[pprev + gi], qy = d.qy[pprev + gi];
+      d.z[pcur + gi] = z1;
+      d.qx[pcur + gi] = qx;
+      d.qy[pcur + gi] = qy;
       d.h[scur + gi] = h1;
       d.h0[scur + gi] = h1;
       d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
@@ -466,9 +971,10 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
         d.fe1[scur + gi] = d.fe1[sprev + gi];
         d.fn1[scur + gi] = d.fn1[sprev + gi];
       }
-      courant_cell(d, h1, d.qx[gi], d.qy[gi], dtc, hm);
+      courant_cell(d, h1, qx, qy, dtc, hm);
     }
     reduce_courant(d, S, dtc, hm);
+    reduce_budget(d, S.budget, bmelt, 0.0);
     return;
   }
 
@@ -485,10 +991,10 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
     unsigned char cl = 0;
     if (r >= 0 && r <= d.nr + 1 && q >= 0 && q <= d.nc + 1) {
       const long long gi = fx_ix(d, r, q);
-      z = d.z[gi];
+      z = d.z[pprev + gi];
       zb = d.zb[gi];
-      qx = d.qx[gi];
-      qy = d.qy[gi];
+      qx = d.qx[pprev + gi];
+      qy = d.qy[pprev + gi];
       if (r >= 1 && r <= d.nr && q >= 1 && q <= d.nc) {
         cl = C_INT;
         if (d.flags[sprev + gi] & FX_F_WALL) cl |= C_WALL;
@@ -563,7 +1069,7 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
   __syncthreads();
 
   // ---- phase D: Loop 3, Loop 4, friction, store, next Courant --------------
-  double dtc = __longlong_as_double(0x7ff0000000000000LL), hm = 0.0;
+  double dtc = __longlong_as_double(0x7ff0000000000000LL), hm = 0.0, bmelt = 0.0, bout = 0.0;
   if (own) {
     const long long gi = fx_ix(d, irow, icol);
     const int sP = sidx(lx + 2, ly + 2);
@@ -573,7 +1079,7 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
     const uint8_t fl = d.flags[sprev + gi];
     const double zb = S.zb[sP];
     const double z1 = S.z[sP];
-    const double zpre = d.z[gi];
+    const double zpre = d.z[pprev + gi];
 
     // add_meteo's h0 (common.cpp:223): the depth after the melt, or the
     // Courant scan's copy of h (main.cpp:305) for cells it skips. Its solute
@@ -582,6 +1088,7 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
     if (melt_on && zb != d.nodata) {
       h0v = fmax(z1 - zb, 0.0);
       if (d.ade) d.hpm[scur + gi] = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
+      bmelt = melt_depth(d, c, gi) * d.arbase;
     }
     // Loop 1 wet time (:69-70)
     if (!(cl & C_DRY)) d.twet[gi] += dtl / 3600;
@@ -596,6 +1103,13 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
       qyfP = S.f[3][fP] * dtl;
     }
     const unsigned char clW = S.cls[sidx(lx + 1, ly + 2)], clS = S.cls[sidx(lx + 2, ly + 1)];
+    if (!wall) {
+      // water leaving the domain this step: through the outflow faces, and
+      // into wall cells (which never take it up, hydrodynamics_calc.cpp:111-117)
+      const unsigned char clE = S.cls[sidx(lx + 3, ly + 2)], clN = S.cls[sidx(lx + 2, ly + 3)];
+      if (irow == d.nr || (clE & C_WALL)) bout += S.f[0][fP] * d.dxy * dtl;
+      if (icol == d.nc || (clN & C_WALL)) bout += S.f[3][fP] * d.dxy * dtl;
+    }
     const double qxfW = ((clW & C_INT) && !(clW & C_WALL)) ? S.f[0][fW] * dtl : 0.0;
     const double qyfS = ((clS & C_INT) && !(clS & C_WALL)) ? S.f[3][fS] * dtl : 0.0;
 
@@ -626,10 +1140,10 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
         qy = qy / den;
       }
     }
-    d.z[gi] = z;
+    d.z[pcur + gi] = z;
     d.h[scur + gi] = h;
-    d.qx[gi] = qx;
-    d.qy[gi] = qy;
+    d.qx[pcur + gi] = qx;
+    d.qy[pcur + gi] = qy;
     d.h0[scur + gi] = h0v;
     d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
     // Fluxes computed this step become the grid values (stale ones are
@@ -660,17 +1174,88 @@ __global__ void __launch_bounds__(NTHREADS) k_hydro(fx_dev d) {
     courant_cell(d, h, qx, qy, dtc, hm);
   }
   reduce_courant(d, S, dtc, hm);
+  reduce_budget(d, S.budget, bmelt, bout);
 }
+
+// Reads the step's fields of the control block (written by k_finalize) into
+// shared memory, then runs the tile in the domain's precision.
+template <bool P32, int BY>
+__device__ __forceinline__ void hydro_block(const fx_dev& d, const fx_tile& tile, HydroSmem<BY>& S,
+                                            StepCtl& sc) {
+  static_assert(sizeof(HydroSmem32<BY>) <= sizeof(HydroSmem<BY>), "FP32 tile state reuses the FP64 one");
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const fx_ctl& g = *d.ctl;
+    sc.dtfl = g.dtfl;
+    sc.meteoi = g.meteoi;
+    sc.meteo_rate = g.meteo_rate;
+    sc.mconc = g.mconc;
+    sc.steps = g.steps;
+    sc.live = g.live;
+    sc.active = g.active;
+  }
+  __syncthreads();
+  const StepCtl c = sc;
+  if (!c.live) return;
+  if constexpr (P32) hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S));
+  else hydro_tile64<BY>(d, c, tile, S);
+}
+
+// Blocks per SM the launch bounds ask for: 512 threads, at most 128
+// registers each.
+template <int BY>
+constexpr int min_blocks() { return 16 / BY; }
+
+// One domain: the descriptor is a kernel parameter (constant bank), so its
+// fields are instruction operands. Block (x, y) is tile (x, y).
+template <bool P32, int BY>
+__global__ void __launch_bounds__(BX * BY, min_blocks<BY>()) k_hydro_one(const __grid_constant__ fx_dev d) {
+  __shared__ HydroSmem<BY> S;
+  __shared__ StepCtl sc;
+  const fx_tile tile{0, (int)blockIdx.x, (int)blockIdx.y, 0};
+  hydro_block<P32, BY>(d, tile, S, sc);
+}
+
+// A batch of domains: one block per entry of the tile table; the block copies
+// its domain's descriptor to shared memory.
+template <bool P32, int BY>
+__global__ void __launch_bounds__(BX * BY, min_blocks<BY>()) k_hydro_batch(const fx_dev* __restrict__ devs,
+                                                                        const fx_tile* __restrict__ tiles) {
+  __shared__ HydroSmem<BY> S;
+  __shared__ fx_dev sd;
+  __shared__ StepCtl sc;
+  const fx_tile tile = tiles[blockIdx.x];
+  {
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(devs + tile.dom);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+    for (int i = tid; i < (int)(sizeof(fx_dev) / 8); i += BX * BY) dst[i] = src[i];
+  }
+  __syncthreads();
+  hydro_block<P32, BY>(sd, tile, S, sc);
+}
+static_assert(sizeof(fx_dev) % 8 == 0, "descriptor copied as 8-byte words");
 
 // Courant scan of the state as uploaded (the scan at the top of the first
 // step). Also used after a host edit of the state.
-__global__ void __launch_bounds__(NTHREADS) k_courant_scan(fx_dev d) {
-  const int irow = 1 + blockIdx.x * BX + threadIdx.x, icol = 1 + blockIdx.y * BY + threadIdx.y;
-  __shared__ HydroSmem S;
+template <int BY>
+__global__ void __launch_bounds__(BX * BY) k_courant_scan(const fx_dev* __restrict__ devs,
+                                                         const fx_tile* __restrict__ tiles) {
+  constexpr int TY = Tile<BY>::TY;
+  __shared__ HydroSmem<BY> S;
+  __shared__ fx_dev sd;
+  const fx_tile tile = tiles[blockIdx.x];
+  if (threadIdx.x == 0 && threadIdx.y == 0) sd = devs[tile.dom];
+  __syncthreads();
+  const fx_dev& d = sd;
+  const int irow = 1 + tile.bx * TX + threadIdx.x, icol = 1 + tile.by * TY + threadIdx.y;
   double dtc = __longlong_as_double(0x7ff0000000000000LL), hm = 0.0;
-  if (irow <= d.nr && icol <= d.nc) {
+  if (threadIdx.x < TX && threadIdx.y < TY && irow <= d.nr && icol <= d.nc) {
     const long long gi = fx_ix(d, irow, icol);
-    courant_cell(d, d.h[fx_slot(d, d.ctl->steps) + gi], d.qx[gi], d.qy[gi], dtc, hm);
+    const long long sl = fx_slot(d, d.ctl->steps), pl = fx_pp(d, d.ctl->steps);
+    if (d.prec32)
+      courant_cell(d, (double)d.h_f[sl + gi], (double)d.qx_f[pl + gi], (double)d.qy_f[pl + gi], dtc, hm);
+    else
+      courant_cell(d, d.h[sl + gi], d.qx[pl + gi], d.qy[pl + gi], dtc, hm);
   }
   reduce_courant(d, S, dtc, hm);
 }
@@ -683,9 +1268,12 @@ __device__ int forcing_row(const float* t, double tim) {
   return -1;
 }
 
-// The clock update of one step, single thread (main.cpp:271-325 and
+// The clock update of one step, one thread per domain (main.cpp:271-325 and
 // common.cpp:195-208).
-__global__ void k_finalize(fx_dev d) {
+__global__ void k_finalize(const fx_dev* __restrict__ devs, int ndom) {
+  const int dom = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dom >= ndom) return;
+  const fx_dev& d = devs[dom];
   fx_ctl& c = *d.ctl;
   c.live = 0;
   if (c.error || c.print_pending || c.finished || c.steps >= c.stop_after) return;
@@ -734,10 +1322,14 @@ __global__ void k_finalize(fx_dev d) {
 }
 
 // Opens a batch of steps whose ADE sweeps run together (fx_ade.cu).
-__global__ void k_batch_begin(fx_dev d) { d.ctl->batch = d.ctl->batch + 1; }
+__global__ void k_batch_begin(const fx_dev* __restrict__ devs, int ndom) {
+  const int dom = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dom < ndom) devs[dom].ctl->batch = devs[dom].ctl->batch + 1;
+}
 
 // Sets the bed flags that never change (NODATA bed) in every slot plane.
-__global__ void k_mark_static(fx_dev d) {
+__global__ void k_mark_static(const fx_dev* __restrict__ devs, int dom) {
+  const fx_dev& d = devs[dom];
   const long long n = d.plane;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int icol = (int)(i / d.ld), irow = (int)(i % d.ld) - FX_ROFF;
@@ -750,19 +1342,118 @@ __global__ void k_mark_static(fx_dev d) {
   }
 }
 
-}  // namespace fx
-
-// Launch helpers used by fx_capi.cu.
-void fx_launch_finalize(const fx_dev& d, cudaStream_t s) { fx::k_finalize<<<1, 1, 0, s>>>(d); }
-void fx_launch_batch_begin(const fx_dev& d, cudaStream_t s) { fx::k_batch_begin<<<1, 1, 0, s>>>(d); }
-void fx_launch_mark_static(const fx_dev& d, cudaStream_t s) { fx::k_mark_static<<<592, 256, 0, s>>>(d); }
-
-void fx_launch_hydro(const fx_dev& d, cudaStream_t s) {
-  dim3 b(fx::BX, fx::BY), g((d.nr + fx::TX - 1) / fx::TX, (d.nc + fx::TY - 1) / fx::TY);
-  fx::k_hydro<<<g, b, 0, s>>>(d);
+// FP32 state: eta = z - zb over the whole grid (ghost ring included), from a
+// staged FP64 z in the field layout, into both planes of eta.
+__global__ void k_eta_from_z(const __grid_constant__ fx_dev d, const double* __restrict__ z) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < d.plane;
+       i += (long long)gridDim.x * blockDim.x)
+    d.eta[i] = d.eta[d.plane + i] = (float)(z[i] - d.zb[i]);
 }
 
-void fx_launch_courant_scan(const fx_dev& d, cudaStream_t s) {
-  dim3 b(fx::BX, fx::BY), g((d.nr + fx::BX - 1) / fx::BX, (d.nc + fx::BY - 1) / fx::BY);
-  fx::k_courant_scan<<<g, b, 0, s>>>(d);
+// FP32 state: the bed differences to the east and north neighbours of every
+// interior cell, rounded once from FP64 (0 on the ghost ring).
+__global__ void k_bed_slopes(const __grid_constant__ fx_dev d) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < d.plane;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int icol = (int)(i / d.ld), irow = (int)(i % d.ld) - FX_ROFF;
+    float sx = 0.0f, sy = 0.0f;
+    if (irow >= 1 && irow <= d.nr && icol >= 1 && icol <= d.nc) {
+      sx = (float)(d.zb[i + 1] - d.zb[i]);
+      sy = (float)(d.zb[i + d.ld] - d.zb[i]);
+    }
+    d.sx[i] = sx;
+    d.sy[i] = sy;
+  }
+}
+
+// Stored water sum(z - zb) * dxy^2 over the interior cells that are not
+// walls (the quantity the update conserves: a cell overdrawn by its
+// neighbours' outflow holds a small negative depth until it refills, where h
+// reads 0) and solute mass sum(c * h) * dxy^2, FP64 block sums added into
+// out[0] and out[1 + k].
+__global__ void __launch_bounds__(256) k_mass(const __grid_constant__ fx_dev d, double* __restrict__ out) {
+  __shared__ double red[8][1 + FX_MAX_CHEM];
+  const long long sl = fx_slot(d, d.ctl->steps), pl = fx_pp(d, d.ctl->steps);
+  double acc[1 + FX_MAX_CHEM];
+  for (int k = 0; k <= FX_MAX_CHEM; ++k) acc[k] = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < d.plane;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int icol = (int)(i / d.ld), irow = (int)(i % d.ld) - FX_ROFF;
+    if (irow < 1 || irow > d.nr || icol < 1 || icol > d.nc) continue;
+    if (d.flags[sl + i] & FX_F_WALL) continue;
+    const double h = d.prec32 ? (double)d.h_f[sl + i] : d.h[sl + i];
+    acc[0] += d.prec32 ? (double)d.eta[pl + i] : d.z[pl + i] - d.zb[i];
+    for (int k = 0; k < d.nchem; ++k)
+      acc[1 + k] += h * (d.prec32 ? (double)d.conc_f[k * d.plane + i] : d.conc[k * d.plane + i]);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int k = 0; k <= d.nchem; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x <= d.nchem) {
+    double v = 0.0;
+    for (int j = 0; j < 8; ++j) v += red[j][threadIdx.x];
+    atomicAdd(&out[threadIdx.x], v * d.arbase);
+  }
+}
+
+}  // namespace fx
+
+// Launch helpers used by fx_capi.cu and fx_batch.cu. `devs` is a device
+// array of ndom domain descriptors; tile tables are built by fx_tiles_of.
+void fx_launch_finalize(const fx_dev* devs, int ndom, cudaStream_t s) {
+  fx::k_finalize<<<(ndom + 127) / 128, 128, 0, s>>>(devs, ndom);
+}
+void fx_launch_batch_begin(const fx_dev* devs, int ndom, cudaStream_t s) {
+  fx::k_batch_begin<<<(ndom + 127) / 128, 128, 0, s>>>(devs, ndom);
+}
+void fx_launch_mark_static(const fx_dev* devs, int dom, cudaStream_t s) {
+  fx::k_mark_static<<<592, 256, 0, s>>>(devs, dom);
+}
+namespace {
+template <int BY>
+void launch_hydro_batch(const fx_dev* devs, const fx_tile* tiles, int ntiles, bool prec32, cudaStream_t s) {
+  if (prec32) fx::k_hydro_batch<true, BY><<<ntiles, dim3(fx::BX, BY), 0, s>>>(devs, tiles);
+  else fx::k_hydro_batch<false, BY><<<ntiles, dim3(fx::BX, BY), 0, s>>>(devs, tiles);
+}
+template <int BY>
+void launch_hydro_one(const fx_dev& d, cudaStream_t s) {
+  const dim3 grid((d.nr + fx::TX - 1) / fx::TX, (d.nc + fx::Tile<BY>::TY - 1) / fx::Tile<BY>::TY);
+  if (d.prec32) fx::k_hydro_one<true, BY><<<grid, dim3(fx::BX, BY), 0, s>>>(d);
+  else fx::k_hydro_one<false, BY><<<grid, dim3(fx::BX, BY), 0, s>>>(d);
+}
+}  // namespace
+
+bool fx_tile_rows_ok(int r) { return r == 4 || r == 8 || r == 16; }
+
+void fx_launch_hydro(const fx_dev* devs, const fx_tile* tiles, int ntiles, bool prec32, int tile_rows,
+                     cudaStream_t s) {
+  if (tile_rows == 4) launch_hydro_batch<4>(devs, tiles, ntiles, prec32, s);
+  else if (tile_rows == 16) launch_hydro_batch<16>(devs, tiles, ntiles, prec32, s);
+  else launch_hydro_batch<8>(devs, tiles, ntiles, prec32, s);
+}
+void fx_launch_hydro_one(const fx_dev& d, cudaStream_t s) {
+  if (d.tile_rows == 4) launch_hydro_one<4>(d, s);
+  else if (d.tile_rows == 16) launch_hydro_one<16>(d, s);
+  else launch_hydro_one<8>(d, s);
+}
+void fx_launch_courant_scan(const fx_dev* devs, const fx_tile* tiles, int ntiles, int tile_rows, cudaStream_t s) {
+  if (tile_rows == 4) fx::k_courant_scan<4><<<ntiles, dim3(fx::BX, 4), 0, s>>>(devs, tiles);
+  else if (tile_rows == 16) fx::k_courant_scan<16><<<ntiles, dim3(fx::BX, 16), 0, s>>>(devs, tiles);
+  else fx::k_courant_scan<8><<<ntiles, dim3(fx::BX, 8), 0, s>>>(devs, tiles);
+}
+void fx_launch_eta_from_z(const fx_dev& d, const double* z, cudaStream_t s) {
+  fx::k_eta_from_z<<<592, 256, 0, s>>>(d, z);
+}
+void fx_launch_bed_slopes(const fx_dev& d, cudaStream_t s) { fx::k_bed_slopes<<<592, 256, 0, s>>>(d); }
+void fx_launch_mass(const fx_dev& d, double* out, cudaStream_t s) { fx::k_mass<<<296, 256, 0, s>>>(d, out); }
+// Appends the tiles of domain `dom` (nr x nc interior cells) to a table.
+void fx_tiles_of(int dom, int nr, int nc, int tile_rows, std::vector<fx_tile>& out) {
+  const int ty = tile_rows - 1;
+  const int gx = (nr + fx::TX - 1) / fx::TX, gy = (nc + ty - 1) / ty;
+  for (int by = 0; by < gy; ++by)
+    for (int bx = 0; bx < gx; ++bx) out.push_back(fx_tile{dom, bx, by, 0});
 }

@@ -22,14 +22,47 @@ struct fx_ctx {
   int ade_strips = 0;
   int ade_blocks = 0;
   int batch_steps = 1;         // steps per batch (ADE sweeps in flight)
+  fx_dev* d_dev = nullptr;     // device copy of d (a batch of one domain)
+  fx_tile* d_tiles = nullptr;  // this domain's hydrodynamic tiles
+  int ntiles = 0, nunits = 0;  // hydrodynamic tiles; ADE units of a full batch
+  bool dev_dirty = true;       // d changed since it was copied to d_dev
+  long long dev_version = 0;   // counts changes of d (batches compare it)
   bool prepared = false;
   bool graph_dirty = true;
   bool store_all_opt = false;
   bool negative_forcing = false;
   cudaGraphExec_t graph_exec = nullptr;
+  // FP32 state: z is held as eta = z - zb. An uploaded z (or the z of the
+  // state when zb is replaced) waits here until fx_prepare converts it with
+  // the bed then on the device.
+  std::vector<double> z_pending;
+  double* d_mass = nullptr;    // fx_mass result: water, then one mass per solute
   // file surface (filled by fx_open_modset)
   double h_min_print = 0.0;
   std::string output_folder;
 };
 
 int fx_fail(fx_ctx* ctx, int code, const char* fmt, ...);
+int fx_sync_dev(fx_ctx* ctx);
+void fx_fill_status(const fx_ctl& k, fx_status* st);
+
+// Launch helpers (fx_hydro.cu, fx_ade.cu). `devs` is a device array of
+// domain descriptors; the *_one forms take one domain's descriptor by value.
+void fx_launch_finalize(const fx_dev* devs, int ndom, cudaStream_t s);
+void fx_launch_batch_begin(const fx_dev* devs, int ndom, cudaStream_t s);
+void fx_launch_mark_static(const fx_dev* devs, int dom, cudaStream_t s);
+void fx_launch_hydro(const fx_dev* devs, const fx_tile* tiles, int ntiles, bool prec32, int tile_rows,
+                     cudaStream_t s);
+void fx_launch_hydro_one(const fx_dev& d, cudaStream_t s);
+void fx_launch_courant_scan(const fx_dev* devs, const fx_tile* tiles, int ntiles, int tile_rows, cudaStream_t s);
+void fx_launch_ade(const fx_dev* devs, const fx_unit* units, int nunits, int nblocks, bool prec32, cudaStream_t s);
+void fx_launch_ade_one(const fx_dev& d, int nunits, int nblocks, cudaStream_t s);
+void fx_launch_eta_from_z(const fx_dev& d, const double* z, cudaStream_t s);
+void fx_launch_bed_slopes(const fx_dev& d, cudaStream_t s);
+void fx_launch_mass(const fx_dev& d, double* out, cudaStream_t s);
+void fx_tiles_of(int dom, int nr, int nc, int tile_rows, std::vector<fx_tile>& out);
+bool fx_tile_rows_ok(int tile_rows);
+void fx_units_of(int dom, int nr, int nchem, int steps, std::vector<fx_unit>& out);
+int fx_ade_rows_per_strip();
+int fx_ade_threads_per_block();
+int fx_ade_max_blocks(int* out);

@@ -34,7 +34,7 @@
 #include "fluxos_gpu.h"
 #include "fx_common.cuh"
 
-void fx_launch_ade(const fx_dev& d, int nstrips, int nblocks, cudaStream_t s);
+void fx_launch_ade(const fx_dev* devs, const fx_unit* units, int nunits, int nblocks, bool prec32, cudaStream_t s);
 int fx_ade_rows_per_strip();
 int fx_ade_threads_per_block();
 int fx_ade_max_blocks(int* out);
@@ -48,6 +48,7 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 constexpr size_t kCtlBytes = (sizeof(fx_ctl) + 255) & ~(size_t)255;  // fx_ctl, rounded up
+constexpr size_t kDevBytes = (sizeof(fx_dev) + 255) & ~(size_t)255;  // fx_dev, rounded up
 
 struct DeviceSetup {
   bool ready = false;
@@ -57,9 +58,14 @@ struct DeviceSetup {
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mutex;
 
-// One sweep with it > 1 (the ADE is skipped on the first solver iteration,
-// ADEsolver_calc.cpp:45) on a fresh epoch.
-__global__ void k_noalloc_ctl(fx_ctl* ctl, double dtfl) {
+// Writes the scratch's control block, domain descriptor and work table: one
+// sweep with it > 1 (the ADE is skipped on the first solver iteration,
+// ADEsolver_calc.cpp:45), one solute, every strip.
+__global__ void k_noalloc_setup(fx_dev d, fx_dev* dst, fx_unit* units, int nstrips, double dtfl) {
+  for (int s = threadIdx.x; s < nstrips; s += blockDim.x) units[s] = fx_unit{0, 0, 0, s};
+  if (threadIdx.x != 0) return;
+  *dst = d;
+  fx_ctl* ctl = d.ctl;
   fx_ctl c = {};
   c.dtfl = dtfl;
   c.live = 1;
@@ -98,9 +104,10 @@ extern "C" int fx_adesolver_noalloc(double* conc, const double* h, const double*
 
   const int rows = fx_ade_rows_per_strip();
   const int nstrips = (nrows + rows - 1) / rows;
+  const size_t unit_bytes = round256((size_t)nstrips * sizeof(fx_unit));
   const size_t prog_bytes = round256((size_t)nstrips * sizeof(unsigned long long));
   const size_t bnd_bytes = (size_t)nstrips * (size_t)(ncols + 2) * 3 * sizeof(double);
-  const size_t need = kCtlBytes + prog_bytes + bnd_bytes;
+  const size_t need = kCtlBytes + kDevBytes + unit_bytes + prog_bytes + bnd_bytes;
   if (need > FX_NOALLOC_SCRATCH_BYTES)
     return fx_fail(nullptr, FX_ERR_ARG,
                    "fx_adesolver_noalloc: a %d x %d grid needs %zu bytes of scratch, more than the %u-byte "
@@ -148,17 +155,20 @@ extern "C" int fx_adesolver_noalloc(double* conc, const double* h, const double*
   d.flags = const_cast<uint8_t*>(flags);
   d.fe1 = const_cast<double*>(fe_1);
   d.fn1 = const_cast<double*>(fn_1);
-  d.ctl = reinterpret_cast<fx_ctl*>(s.scratch);
-  d.ade_prog = reinterpret_cast<unsigned long long*>(s.scratch + kCtlBytes);
-  d.ade_bnd = reinterpret_cast<double*>(s.scratch + kCtlBytes + prog_bytes);
+  unsigned char* p = s.scratch;
+  d.ctl = reinterpret_cast<fx_ctl*>(p);
+  fx_dev* d_dev = reinterpret_cast<fx_dev*>(p + kCtlBytes);
+  fx_unit* d_units = reinterpret_cast<fx_unit*>(p + kCtlBytes + kDevBytes);
+  d.ade_prog = reinterpret_cast<unsigned long long*>(p + kCtlBytes + kDevBytes + unit_bytes);
+  d.ade_bnd = reinterpret_cast<double*>(p + kCtlBytes + kDevBytes + unit_bytes + prog_bytes);
 
-  k_noalloc_ctl<<<1, 1, 0, st>>>(d.ctl, dtfl);
+  k_noalloc_setup<<<1, 128, 0, st>>>(d, d_dev, d_units, nstrips, dtfl);
   e = cudaMemsetAsync(d.ade_prog, 0, prog_bytes, st);
   if (e != cudaSuccess) return fx_fail(nullptr, FX_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
   const int per_block = fx_ade_threads_per_block() / 32;
   int nblocks = (nstrips + per_block - 1) / per_block;
   if (nblocks > s.max_blocks) nblocks = s.max_blocks;
-  fx_launch_ade(d, nstrips, nblocks, st);
+  fx_launch_ade(d_dev, d_units, nstrips, nblocks, false, st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fx_fail(nullptr, FX_ERR_CUDA, "ADE sweep launch failed: %s", cudaGetErrorString(e));
   int err = 0;

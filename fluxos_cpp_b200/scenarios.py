@@ -254,3 +254,98 @@ def wet_start(sc: Scenario, depth: float = 0.05, seed: int = 7, fill_depressions
     sc.init_qy = np.zeros_like(h)
     sc.init_conc = [np.where(h > 2 * depth, 1.0, 0.0) for _ in range(sc.nchem)]
     return sc
+
+
+def dambreak_scenario(n: int = 2048, dxy: int = 1, radius: float = 300.0, depth: float = 2.0,
+                      base: float = 10.0, manning: float = 0.02, horizon: float = 600.0) -> Scenario:
+    """Circular dam break on a flat bed: ``depth`` m of water inside ``radius``
+    m of the centre, dry outside, uniform Manning n, no melt, two solutes
+    (unit concentration inside the dam, D = 0.1 and 1.0 m^2/s). The bed sits
+    at ``base`` m because a DEM value of 0 marks a wall cell."""
+    dem = np.full((n, n), base, dtype=np.float32)
+    c = (np.arange(n) + 0.5) * dxy - 0.5 * n * dxy
+    rr = np.sqrt(c[:, None] ** 2 + c[None, :] ** 2)
+    inside = rr < radius
+    sc = Scenario(name=f"dambreak{n}", dem=dem, dxy=dxy, meteo=((0.0, 0.0, 0.0),), horizon=horizon,
+                  print_step=int(horizon), ks=0.001, ade=True, d_coef=0.1, d_coefs=[0.1, 1.0])
+    sc.manning = np.full((n, n), manning)
+    sc.init_h = np.where(inside, depth, 0.0)
+    sc.init_qx = np.zeros((n, n))
+    sc.init_qy = np.zeros((n, n))
+    sc.init_conc = [inside.astype(np.float64), inside.astype(np.float64)]
+    sc.extra["radius"] = radius
+    return sc
+
+
+def forcing_table(sc: Scenario) -> np.ndarray:
+    """The forcing table as read_meteo fills GlobVar::meteo (3 x 2000 float,
+    rows from 1), with the guard and horizon rows of write_meteo."""
+    tab = np.zeros((3, 2000), dtype=np.float32)
+    rows = list(sc.meteo) + [(GUARD_TIME, 0.0, 0.0), (sc.horizon, 0.0, 0.0)]
+    for a, (t, r, c) in enumerate(rows, start=1):
+        tab[:, a] = (t, r, c)
+    return tab
+
+
+def full_grid(sc: Scenario, interior: np.ndarray, fill: float = 0.0) -> np.ndarray:
+    """An interior (nrows, ncols) array as a GlobVar grid (ncols+2, nrows+2)."""
+    g = np.full((sc.ncols + 2, sc.nrows + 2), fill)
+    g[1:-1, 1:-1] = np.asarray(interior, dtype=np.float64).T
+    return g
+
+
+def make_domain(sc: Scenario, *, precision: str = "fp64", steps_in_flight: int = 8):
+    """A GPU domain of the scenario without its files: the reference's
+    initiation of the DEM (fx_initiate), the forcing, the extension grids and
+    the scenario's wet start, if any."""
+    import fluxos_cpp_b200 as fx
+    d = fx.Domain(sc.nrows, sc.ncols, sc.dxy, nchem=sc.nchem, nodata=float(sc.nodata), hdry=sc.ks,
+                  ntim=sc.horizon, print_step=sc.print_step, print_next=sc.print_step, ade=sc.ade,
+                  d_coef=list(sc.d_coefs) if sc.d_coefs else [sc.d_coef],
+                  steps_in_flight=steps_in_flight, precision=precision)
+    d.initiate(full_grid(sc, sc.dem.astype(np.float64)))
+    d.set_forcing(forcing_table(sc))
+    if sc.melt_mult is not None:
+        d.set_melt_field(full_grid(sc, sc.melt_mult, 1.0))
+    if sc.manning is not None:
+        d.set_manning(full_grid(sc, sc.manning, 0.0))
+    if sc.init_h is not None:
+        zb = d.download("zb")
+        h = full_grid(sc, sc.init_h)
+        d.upload("z", zb + h)
+        d.upload("h", h)
+        if sc.init_qx is not None:
+            d.upload("qx", full_grid(sc, sc.init_qx))
+        if sc.init_qy is not None:
+            d.upload("qy", full_grid(sc, sc.init_qy))
+        for k, c in enumerate(sc.init_conc or []):
+            d.upload("conc" if k == 0 else f"conc{k}", full_grid(sc, c))
+        fl = d.download_flags()
+        ld = full_grid(sc, np.where(sc.init_h > sc.ks, 0.0, 1.0))
+        d.upload_flags(ld, fl["wall"])
+    d.prepare()
+    return d
+
+
+def ensemble_scenarios(count: int = 64, seed: int = 3, n_min: int = 256, n_max: int = 2048,
+                       dxy: int = 2, horizon: float = 21600.0, wet: bool = True) -> List[Scenario]:
+    """The batched-ensemble configuration: `count` square grids with sizes
+    log-uniform in [n_min, n_max] (seeded), each with its own fractal DEM as
+    in the large-domain configuration, a uniform melt rate U[5, 50] mm/day,
+    Manning n U[0.03, 0.15] per cell, one solute, a 6 h horizon and (with
+    `wet`) the wet start of wet_start."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(n_min), math.log(n_max), size=count)).round().astype(int)
+    rates = rng.uniform(5.0, 50.0, size=count)
+    seeds = rng.integers(0, 2**31 - 1, size=count)
+    out = []
+    for i in range(count):
+        n, s = int(sizes[i]), int(seeds[i])
+        sc = Scenario(name=f"ens{i}_{n}", dem=fractal_dem(n, n, dxy, s), dxy=dxy,
+                      meteo=((0.0, float(rates[i]), 1.0), (horizon, float(rates[i]), 1.0)),
+                      horizon=horizon, print_step=3600, ks=0.001, ade=True, d_coef=0.01)
+        sc.manning = np.random.default_rng(s + 1).uniform(0.03, 0.15, size=(n, n))
+        if wet:
+            wet_start(sc, depth=0.005, seed=s + 2)
+        out.append(sc)
+    return out

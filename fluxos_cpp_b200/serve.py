@@ -1,0 +1,210 @@
+"""Continuous batching of scenario solves on one GPU.
+
+The reference runs one domain per process to the end of its forcing
+(main.cpp:271-470). Here a request is such a run: a scenario (terrain,
+forcing, horizon, solutes) to be advanced from its start state to its
+horizon. The loop keeps every admitted scenario's state resident on the GPU
+as a member of one fx_batch, so all of them advance through the same
+launches, each with its own clock and dt:
+
+* admission: requests are taken in arrival order as soon as they have
+  arrived and their device footprint (fx_footprint) fits under the cap
+  beside the members already resident;
+* stepping: the batch advances a chunk of steps at a time; members whose
+  output falls due stop inside the chunk and are acknowledged (optionally
+  written out) before the next one;
+* retirement: a member whose clock passed its horizon leaves the batch
+  between chunks, its result is taken and its memory freed, which makes room
+  for the next arrivals.
+
+Scenario inputs (terrain and fields) are generated on host threads ahead of
+admission so the GPU does not wait for them. Latency of a request is the
+time from its arrival to its retirement.
+"""
+from __future__ import annotations
+
+import collections
+import concurrent.futures as cf
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional
+
+import numpy as np
+
+import fluxos_cpp_b200 as fx
+from fluxos_cpp_b200 import scenarios as S
+
+
+@dataclass
+class Request:
+    """One scenario solve. `make` builds the Scenario (called on a host
+    thread); `cells`, `nchem` and `extension_grids` size the admission."""
+
+    rid: int
+    arrival: float
+    make: Callable[[], S.Scenario]
+    nrows: int
+    ncols: int
+    nchem: int = 1
+    extension_grids: int = 2
+    precision: str = "fp32"
+    steps_in_flight: int = 4
+    # filled in by the server
+    admitted: Optional[float] = None
+    done: Optional[float] = None
+    steps: int = 0
+    status: Optional[dict] = None
+    water: Optional[float] = None
+    state: Dict[str, np.ndarray] = field(default_factory=dict)
+
+    @property
+    def cells(self) -> int:
+        return self.nrows * self.ncols
+
+    @property
+    def latency(self) -> Optional[float]:
+        return None if self.done is None else self.done - self.arrival
+
+
+class Server:
+    """The request loop. `keep` names fields to download at retirement
+    (e.g. ("h", "conc")); `on_output(req, domain)` runs for every due output
+    before it is acknowledged."""
+
+    def __init__(self, cap_bytes: float = 150e9, chunk_steps: int = 32, keep=(),
+                 on_output: Optional[Callable] = None, host_threads: int = 4,
+                 clock: Callable[[], float] = time.perf_counter):
+        self.cap = float(cap_bytes)
+        self.chunk = int(chunk_steps)
+        self.keep = tuple(keep)
+        self.on_output = on_output
+        self.clock = clock
+        self.pool = cf.ThreadPoolExecutor(max_workers=host_threads)
+        self.batch = fx.Batch()
+        self.active: List[tuple] = []  # (request, domain, bytes)
+        self.used = 0
+        self.peak_used = 0
+        self.peak_members = 0
+        self.cell_updates = 0
+        self.gpu_busy = 0.0
+
+    def close(self) -> None:
+        for _, d, _ in self.active:
+            d.close()
+        self.active = []
+        self.batch.close()
+        self.pool.shutdown(wait=False)
+
+    @staticmethod
+    def footprint(r: Request) -> int:
+        return fx.footprint(r.nrows, r.ncols, nchem=r.nchem, precision=r.precision,
+                            steps_in_flight=r.steps_in_flight, extension_grids=r.extension_grids)
+
+    def _retire(self, i: int, now: float) -> None:
+        r, d, nbytes = self.active.pop(i)
+        self.batch.remove(d)
+        r.status = d.status()
+        r.steps = int(r.status["steps"])
+        r.water = d.mass()[0]
+        for k in self.keep:
+            r.state[k] = d.download(k)
+        d.close()
+        self.used -= nbytes
+        r.done = now
+
+    def run(self, requests: List[Request]) -> dict:
+        """Serve `requests` (arrival times in seconds from the call) to the
+        end; returns throughput and latency figures."""
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        futures = {}
+        t0 = self.clock()
+        lookahead = 8
+        while pending or self.active:
+            now = self.clock() - t0
+            # host-side input generation ahead of admission
+            for r in list(pending)[:lookahead]:
+                if r.rid not in futures:
+                    futures[r.rid] = self.pool.submit(r.make)
+            # admission in arrival order while the footprint fits
+            while pending and pending[0].arrival <= now:
+                r = pending[0]
+                need = self.footprint(r)
+                if self.active and self.used + need > self.cap:
+                    break
+                sc = futures.pop(r.rid).result()
+                d = S.make_domain(sc, precision=r.precision, steps_in_flight=r.steps_in_flight)
+                self.batch.add(d)
+                nbytes = d.device_bytes()
+                self.active.append((r, d, nbytes))
+                self.used += nbytes
+                self.peak_used = max(self.peak_used, self.used)
+                self.peak_members = max(self.peak_members, len(self.active))
+                r.admitted = self.clock() - t0
+                pending.popleft()
+                now = self.clock() - t0
+            if not self.active:
+                if pending:
+                    time.sleep(max(0.0, min(0.002, pending[0].arrival - (self.clock() - t0))))
+                continue
+            before = [st["steps"] for st in (d.status() for _, d, _ in self.active)]
+            g0 = self.clock()
+            sts = self.batch.step(self.chunk)
+            self.gpu_busy += self.clock() - g0
+            now = self.clock() - t0
+            for (r, d, _), st, s0 in zip(self.active, sts, before):
+                self.cell_updates += (st["steps"] - s0) * r.cells
+            for i in range(len(self.active) - 1, -1, -1):
+                r, d, _ = self.active[i]
+                st = sts[i]
+                if st["device_error"]:
+                    raise fx.FluxosError(-5, f"request {r.rid}: device error")
+                if st["print_pending"]:
+                    if self.on_output:
+                        self.on_output(r, d)
+                    d.print_done()
+                if st["finished"]:
+                    self._retire(i, now)
+        wall = self.clock() - t0
+        lat = np.array([r.latency for r in requests if r.latency is not None])
+        return {"requests": len(requests), "wall_s": wall,
+                "cell_updates": self.cell_updates,
+                "cell_updates_per_s": self.cell_updates / wall if wall > 0 else 0.0,
+                "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
+                "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
+                "peak_device_bytes": self.peak_used, "peak_members": self.peak_members,
+                "batch_step_s": self.gpu_busy}
+
+
+def poisson_requests(rate: float, duration: float, seed: int, *, n_min: int = 128, n_max: int = 4096,
+                     horizon_h=(1.0, 12.0), horizon_scale: float = 1.0, nchem=(1, 3),
+                     precision: str = "fp32", dxy: int = 2, wet: bool = True) -> List[Request]:
+    """Seeded request stream of the serving configuration: Poisson arrivals,
+    square grids log-uniform in [n_min, n_max], horizon uniform in hours
+    (times `horizon_scale`), 1-3 solutes, terrain and melt field as the
+    large-domain configuration (fractal DEM, melt 5-40 mm/day field, Manning
+    n U[0.03, 0.15]) and a wet start."""
+    rng = np.random.default_rng(seed)
+    out, t, rid = [], 0.0, 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        hor = float(rng.uniform(*horizon_h)) * 3600.0 * horizon_scale
+        k = int(rng.integers(nchem[0], nchem[1] + 1))
+        s = int(rng.integers(0, 2**31 - 1))
+
+        def make(n=n, hor=hor, k=k, s=s):
+            sc = S.fractal_scenario(n, dxy=dxy, seed=s, melt_seed=s + 1, extensions=True, horizon=hor)
+            sc.print_step = max(1, int(hor))
+            if k > 1:
+                sc.d_coefs = [0.01 * (10 ** j) for j in range(k)]
+            if wet:
+                S.wet_start(sc, depth=0.005, seed=s + 2)
+            return sc
+
+        out.append(Request(rid=rid, arrival=t, make=make, nrows=n, ncols=n, nchem=k,
+                           precision=precision))
+        rid += 1
+    return out

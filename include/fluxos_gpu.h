@@ -64,6 +64,13 @@ typedef struct fx_params {
   int volrat_mode;   /* domain-edge weir: 0 = weir formula (default), 1 = closed */
   double d_coef[FX_MAX_CHEM]; /* dispersion coefficient per solute */
   int steps_in_flight; /* steps whose ADE sweeps run in one launch, 1..15 (0 = 8) */
+  int precision;       /* 0 = FP64, the reference's arithmetic (default);
+                          1 = FP32 state: the depth above the bed eta = z - zb and
+                          the bed's differences to the east and north neighbours
+                          are stored instead of z, flux/update/ADE arithmetic is
+                          FP32; the clock, the wet/dry threshold tests and the
+                          water budget stay FP64. Not bit-compatible with the
+                          reference: see tests/test_gpu_fp32.py for its error. */
 } fx_params;
 
 /* Clock and status read back from the device. */
@@ -78,6 +85,10 @@ typedef struct fx_status {
   int finished;         /* tim > ntim: the run is over */
   int device_error;     /* nonzero when a kernel gave up a bounded wait */
   int forcing_overrun;  /* the forcing table had no row later than tim */
+  double budget_melt;   /* water added by the forcing since creation [m^3], FP64 */
+  double budget_out;    /* water that left through the outflow faces (E face of
+                           irow = NROWS, N face of icol = NCOLS) or into wall
+                           cells since creation [m^3], FP64 */
 } fx_status;
 
 /* --- context ------------------------------------------------------------ */
@@ -85,6 +96,10 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out);
 void fx_destroy(fx_ctx* ctx);
 const char* fx_last_error(const fx_ctx* ctx); /* ctx may be NULL: last global error */
 int fx_device_bytes(const fx_ctx* ctx, long long* bytes); /* device memory held */
+/* Device memory fx_create would take for this grid and these parameters,
+ * plus `extension_grids` per-cell extension grids (fx_set_manning,
+ * fx_set_melt_field): the figure an admission policy sizes against. */
+int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long long* bytes);
 
 /* --- state ---------------------------------------------------------------
  * Field names: "z" "zb" "h" "qx" "qy" "twet" "h0" "fe_1" "fe_2" "fe_3"
@@ -107,7 +122,9 @@ int fx_set_manning(fx_ctx* ctx, const double* n_grid);
 int fx_set_melt_field(fx_ctx* ctx, const double* mult_grid);
 /* Options: "store_all_fluxes" (1 keeps fe_2/fe_3/fn_2/fn_3 current on the
  * device every step; 0, the default, skips those stores for cells that end a
- * step wet, whose values are never read back by a later step). */
+ * step wet, whose values are never read back by a later step);
+ * "tile_rows" (4, 8 or 16: hydrodynamic tiles of 31 x (tile_rows - 1) cells,
+ * 32 x tile_rows threads; default 8). Results do not depend on tile_rows. */
 int fx_set_option(fx_ctx* ctx, const char* name, long long value);
 int fx_prepare(fx_ctx* ctx);
 
@@ -125,6 +142,45 @@ void* fx_stream(fx_ctx* ctx);
  * context's stream, plus the summed time of the hydro and ADE kernels
  * measured launch by launch (for roofline accounting). */
 int fx_time_steps(fx_ctx* ctx, int nsteps, double* ms_total, double* ms_hydro, double* ms_ade);
+/* Stored water sum(h) * dxy^2 over the interior cells [m^3] and, when
+ * solute_mass is not NULL, the stored mass sum(conc * h) * dxy^2 of each of
+ * the nchem solutes, summed on the device in FP64. With the budget of
+ * fx_status, water(t) - water(0) = budget_melt - budget_out up to rounding. */
+int fx_mass(fx_ctx* ctx, double* water, double* solute_mass);
+/* Autotuner: runs trial_steps real steps with each tile shape (tile_rows 4,
+ * 8, 16), keeps the one whose hydrodynamic kernel took least time per step
+ * and returns it in *tile_rows (may be NULL). */
+int fx_autotune(fx_ctx* ctx, int trial_steps, int* tile_rows);
+
+/* --- batches --------------------------------------------------------------
+ * No counterpart in the reference (it runs one domain per process). A batch
+ * steps several contexts together: one CUDA graph per batch of steps holds
+ * the clock updates of all members, one hydrodynamic launch over all their
+ * tiles per step and one ADE launch over all their solute strips, so small
+ * and large domains share the GPU. Every member keeps its own clock, dt,
+ * forcing and outputs, and stops on its own (output due, run over, step
+ * budget spent). Members are added or removed between fx_batch_step calls;
+ * while in a batch, a context is stepped only through it (its upload,
+ * download and output calls stay valid between batch steps). */
+typedef struct fx_batch fx_batch;
+int fx_batch_create(fx_batch** out);
+void fx_batch_destroy(fx_batch* b);
+const char* fx_batch_last_error(const fx_batch* b);
+int fx_batch_add(fx_batch* b, fx_ctx* ctx);
+int fx_batch_remove(fx_batch* b, fx_ctx* ctx);
+int fx_batch_size(const fx_batch* b);
+/* Up to nsteps steps of every member; st (may be NULL) receives the members'
+ * status in the order they were added. */
+int fx_batch_step(fx_batch* b, int nsteps, fx_status* st);
+void* fx_batch_stream(fx_batch* b);
+/* Options of the batch's launches: "tile_rows" (4, 8, 16, as for
+ * fx_set_option) and "steps_in_flight" (upper bound on the steps per graph,
+ * 1..15; the members' own steps_in_flight bound it too). */
+int fx_batch_set_option(fx_batch* b, const char* name, long long value);
+/* Autotuner of the batch: tries each tile shape, then each steps-in-flight
+ * bound, for trial_steps real steps of all members, keeps the fastest
+ * (cell-steps per second) and returns the choice (pointers may be NULL). */
+int fx_batch_autotune(fx_batch* b, int trial_steps, int* tile_rows, int* steps_in_flight);
 
 /* --- allocation-free ADE sweep -------------------------------------------
  * No counterpart in the reference. For callers that cannot call cudaMalloc

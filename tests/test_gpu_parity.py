@@ -78,6 +78,31 @@ def test_random_patchwork_parity(nr, nc, seed, mode, tmp_path):
     d.close()
 
 
+@pytest.mark.parametrize("tile_rows", [8, 16])
+def test_many_waves_of_tiles_parity(tile_rows, tmp_path):
+    """A grid with far more tiles than the GPU holds at once (a 1,000 x 700
+    grid is 33 x 117 tiles of 31 x 7 cells): tiles that start after their
+    neighbours have finished must still read the neighbours' state from
+    before the step. 40 steps against the oracle."""
+    nr, nc, seed = 1000, 700, 17
+    sc = _random_scenario(nr, nc, seed)
+    sc.write(str(tmp_path))
+    ora = P.OracleRun(str(tmp_path), sc, 0)
+    rng = np.random.default_rng(seed + 1)
+    h = np.where(rng.random((nr, nc)) < 0.8, rng.uniform(0, 0.2, (nr, nc)), 0.0)
+    qx = rng.normal(0, 0.01, (nr, nc)) * (h > 0)
+    qy = rng.normal(0, 0.01, (nr, nc)) * (h > 0)
+    ora.apply_wet_start(h, qx, qy, [np.where(h > 0.1, 1.0, 0.0)])
+    d = GP.domain_from_oracle(ora, sc, 0)
+    d.set_option("tile_rows", tile_rows)
+    for n in (3, 37):
+        GP.advance_oracle(ora, n)
+        GP.advance_domain(d, n)
+        res, bad = GP.compare(ora, d, sc)
+        assert not bad, (n, bad)
+    d.close()
+
+
 def test_flux_store_skipping_changes_nothing(tmp_path):
     """Skipping the fe_2/fe_3/fn_2/fn_3 stores of cells that end a step wet
     gives the same state as storing every flux."""
