@@ -214,7 +214,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
   } else {
     const size_t pf = (size_t)d.plane * sizeof(float);
     float** fields[] = {&d.sx, &d.sy, &d.twet_f, &d.fe2_f, &d.fe3_f, &d.fn2_f, &d.fn3_f};
-    float** pair_fields[] = {&d.eta, &d.qx_f, &d.qy_f};
+    float** pair_fields[] = {&d.eta, &d.eta_lo, &d.qx_f, &d.qy_f};
     float** slot_fields[] = {&d.h_f, &d.h0_f, &d.hpm_f, &d.fe1_f, &d.fn1_f};
     if ((rc = dev_alloc(c, (void**)&d.zb, (size_t)d.plane * sizeof(double))) != FX_OK) goto fail;
     for (float** f : fields)
@@ -320,7 +320,7 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
   const long long gx = (g->nrows + 30) / 31, gy = (g->ncols + 6) / 7;
   long long b = 0;
   if (p->precision == 1)
-    b += plane * (8 + 7 * 4 + 3 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids);
+    b += plane * (8 + 7 * 4 + 4 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids);
   else
     b += plane * (6 * 8 + 3 * 2 * 8 + 5 * 8 * nslot + 8LL * g->nchem + 8LL * extension_grids);
   b += plane * nslot;                                   // flags
@@ -376,12 +376,13 @@ static int get_z32(fx_ctx* c, double* host) {
     std::copy(c->z_pending.begin(), c->z_pending.end(), host);
     return FX_OK;
   }
-  std::vector<double> eta(n);
+  std::vector<double> eta(n), lo(n);
   int rc = read_ctl(c);
   if (!rc) rc = get_grid(c, c->d.zb, false, host);
   if (!rc) rc = get_grid(c, c->d.eta + fx_pp(c->d, c->ctl_host->steps), true, eta.data());
+  if (!rc) rc = get_grid(c, c->d.eta_lo + fx_pp(c->d, c->ctl_host->steps), true, lo.data());
   if (rc) return rc;
-  for (size_t i = 0; i < n; ++i) host[i] += eta[i];
+  for (size_t i = 0; i < n; ++i) host[i] += eta[i] + lo[i];
   return FX_OK;
 }
 

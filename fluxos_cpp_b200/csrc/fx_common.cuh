@@ -100,8 +100,8 @@ struct fx_dev {
   // state. h, h0, fe1, fn1 and flags hold `nslot` planes each: the state
   // after step n lives in plane n % nslot, so the ADE sweep of a step can run
   // after the hydrodynamics of the following steps (fx_ade.cu). z, qx, qy
-  // (eta, qx_f, qy_f) hold two planes: the state after step n is in plane
-  // n & 1 (fx_pp).
+  // (eta, eta_lo, qx_f, qy_f) hold two planes: the state after step n is in
+  // plane n & 1 (fx_pp).
   int nslot;
   int pad3_;
   double *z, *zb, *h, *qx, *qy, *twet, *h0;
@@ -123,10 +123,14 @@ struct fx_dev {
   // above the bed eta = z - zb is stored, and the bed enters only through
   // its differences to the east and north neighbours (sx = zb(E) - zb(P),
   // sy = zb(N) - zb(P)), so water-surface differences are sx + (eta_E -
-  // eta_P) and thin films keep their digits. zb stays FP64 for output.
+  // eta_P) and thin films keep their digits. The depth is held compensated,
+  // as the pair (eta, eta_lo) with eta + eta_lo exact and |eta_lo| at most
+  // half an ulp of eta: flux arithmetic reads eta alone, updates add to the
+  // pair without rounding loss, and the wet/dry threshold tests compare
+  // eta + eta_lo in FP64. zb stays FP64 for output.
   int prec32;
   int pad4_;
-  float *eta, *sx, *sy, *qx_f, *qy_f, *twet_f;
+  float *eta, *eta_lo, *sx, *sy, *qx_f, *qy_f, *twet_f;
   float *h_f, *h0_f, *hpm_f, *fe1_f, *fn1_f;  // nslot planes each
   float *fe2_f, *fe3_f, *fn2_f, *fn3_f;
   float* conc_f;                              // nchem planes
@@ -175,6 +179,19 @@ __host__ __device__ inline long long fx_ix(const fx_dev& d, int irow, int icol) 
 __host__ __device__ inline long long fx_slot(const fx_dev& d, long long step) {
   return (step % d.nslot) * d.plane;
 }
+
+// Compensated FP32 depth: (hi, lo) += x with no rounding loss (Knuth's
+// two-sum, exact in round-to-nearest without contraction), renormalised so
+// that |lo| <= ulp(hi) / 2.
+__host__ __device__ inline void fx_dd_add(float& hi, float& lo, float x) {
+  const float s = hi + x;
+  const float bb = s - hi;
+  const float err = (hi - (s - bb)) + (x - bb);
+  const float t = lo + err;
+  hi = s + t;
+  lo = t - (hi - s);
+}
+__host__ __device__ inline double fx_dd_val(float hi, float lo) { return (double)hi + (double)lo; }
 
 // Offset of the plane of z (eta), qx, qy that holds the state after step n:
 // these fields have two planes, so a step reads one while it writes the

@@ -467,6 +467,7 @@ __device__ void reduce_budget(const fx_dev& d, double* red, double melt, double 
 
 __device__ __forceinline__ double melt_depth(const fx_dev& d, const StepCtl& c, long long gi) {
   if (d.melt_mult) return (double)c.meteo_rate * d.melt_mult[gi] / (1000. * 3600. * 24.) * c.dtfl;
+  if (d.melt_mult_f) return (double)c.meteo_rate * (double)d.melt_mult_f[gi] / (1000. * 3600. * 24.) * c.dtfl;
   return c.meteoi;
 }
 
@@ -478,15 +479,17 @@ __device__ __forceinline__ double melt_depth(const fx_dev& d, const StepCtl& c, 
 //   ze - zp = sx(P) + (eta_E - eta_P),  zp - zbpe = eta_P - sx(P)/2,
 //   ze - zbpe = eta_E + sx(P)/2,        h = max(0, eta),
 // and likewise to the north with sy. Flux, update and friction arithmetic is
-// FP32; the wet/dry threshold tests compare in FP64, the Courant candidates
-// and the water budget are FP64.
+// FP32 on the high part of the compensated depth; the branch tests on
+// near-zero depths (wet/dry, the face-depth thresholds of both solvers) and
+// the signs of near-zero surface differences are decided in FP64 on the
+// compensated depth; the Courant candidates and the water budget are FP64.
 
 template <int BY>
 struct HydroSmem32 {
   static constexpr int NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX, NW = Tile<BY>::NTHREADS / 32;
   double budget[2 * NW];
   double red_dt[NW], red_h[NW];
-  float eta[NSTEN], sx[NSTEN], sy[NSTEN], qx[NSTEN], qy[NSTEN];
+  float eta[NSTEN], eta_lo[NSTEN], sx[NSTEN], sy[NSTEN], qx[NSTEN], qy[NSTEN];
   float f[6][NFLUX];
   unsigned char cls[NSTEN];
   short wet_list[NFLUX], dry_list[NFLUX], stale_list[NFLUX];
@@ -514,6 +517,9 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   float volrat = d.volrat_mode == 0 ? __int_as_float(0x7f800000) : 0.0f;
   const bool ldp_dry = S.cls[P] & C_DRY, lde_dry = S.cls[E] & C_DRY, ldn_dry = S.cls[N] & C_DRY;
   const float etap = S.eta[P], sxp = S.sx[P], syp = S.sy[P];
+  // compensated depths for the branch tests (FP64, as the FP64 path decides them)
+  const double dP = fx_dd_val(etap, S.eta_lo[P]), dE = fx_dd_val(S.eta[E], S.eta_lo[E]);
+  const double dN = fx_dd_val(S.eta[N], S.eta_lo[N]);
   float qp = S.qx[P], qe = S.qx[E], qn = S.qx[N];
   float rw = S.qy[W], rp = S.qy[P], re = S.qy[E], rn = S.qy[N];
   const float hp = fmaxf(0.0f, etap);
@@ -531,8 +537,8 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   if (lde_dry) {
     hme = fmaxf(0.0f, etap - .5f * sxp);
     he = qe = re = 0.0f;
-    if ((double)hme > hdry) {
-      if (dze >= 0.0f) {
+    if (fmax(0.0, dP - .5 * (double)sxp) > hdry) {
+      if ((double)sxp + (dE - dP) >= 0.0) {
         qme = rme = 0.0f;
       } else {
         dze = fminf(fabsf(dze), hme);
@@ -549,8 +555,8 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   if (ldn_dry) {
     hmn = fmaxf(0.0f, etap - .5f * syp);
     hn = qn = rn = 0.0f;
-    if ((double)hmn > hdry) {
-      if (dzn >= 0.0f) {
+    if (fmax(0.0, dP - .5 * (double)syp) > hdry) {
+      if ((double)syp + (dN - dP) >= 0.0) {
         qmn = rmn = 0.0f;
       } else {
         dzn = fminf(fabsf(dzn), hmn);
@@ -586,7 +592,7 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   float fe1r = 0.f, fe2r = 0.f, fe3r = 0.f, fn1r = 0.f, fn2r = 0.f, fn3r = 0.f;
   if (lroe) {
     float cc;
-    if ((double)hme > hdry) {
+    if (.5 * (fmax(0.0, dP) + fmax(0.0, dE)) > hdry) {
       float dzea = fabsf(dze);
       if (dzea > 0.5f * hme) {
         dzea = fminf(dzea, fabsf(he - hp));
@@ -601,7 +607,7 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
     fe1r = -((c2 * c3a - c2a * c3) * dze + (c2a - c3a) * dqe) * cc;
     fe2r = -(c2 * c3 * (c3a - c2a) * dze + (c2a * c2 - c3a * c3) * dqe) * cc;
     fe3r = -(vme * (c2 * c3a - 2.f * cme * c1a - c2a * c3) * dze + vme * (c2a - c3a) * dqe + 2.f * cme * c1a * dre) * cc;
-    if (!ldp_dry && (double)hmn > hdry) {
+    if (!ldp_dry && .5 * (fmax(0.0, dP) + fmax(0.0, dN)) > hdry) {
       float dzna = fminf(fabsf(dzn), fabsf(hn - hp));
       dzn = copysignf(dzna, dzn);
       cc = .25f / cmn;
@@ -659,13 +665,15 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
   float volrat = d.volrat_mode == 0 ? __int_as_float(0x7f800000) : 0.0f;
   const bool lde_dry = S.cls[E] & C_DRY, ldn_dry = S.cls[N] & C_DRY;
   const float etap = S.eta[P], etae = S.eta[E], etan = S.eta[N], sxp = S.sx[P], syp = S.sy[P];
+  const double dP = fx_dd_val(etap, S.eta_lo[P]), dE = fx_dd_val(etae, S.eta_lo[E]);
+  const double dN = fx_dd_val(etan, S.eta_lo[N]);
   const float he = fmaxf(0.0f, etae), hn = fmaxf(0.0f, etan);
   float dze = sxp + (etae - etap), dzn = syp + (etan - etap);
   float fe1 = 0.f, fe2 = 0.f, fe3 = 0.f, fn1 = 0.f, fn2 = 0.f, fn3 = 0.f;
   if (!lde_dry) {
     float hme = fmaxf(0.0f, etae + .5f * sxp);
-    if ((double)hme > d.hdry) {
-      if (dze <= 0.0f) {
+    if (fmax(0.0, dE + .5 * (double)sxp) > d.hdry) {
+      if ((double)sxp + (dE - dP) <= 0.0) {
         fe2 = .5f * gaccl * hme * hme;
       } else {
         dze = fminf(fabsf(dze), hme);
@@ -680,8 +688,8 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
   }
   if (!ldn_dry) {
     float hmn = fmaxf(0.0f, etan + .5f * syp);
-    if ((double)hmn > d.hdry) {
-      if (dzn <= 0.0f) {
+    if (fmax(0.0, dN + .5 * (double)syp) > d.hdry) {
+      if ((double)syp + (dN - dP) <= 0.0) {
         fn3 = .5f * gaccl * hmn * hmn;
       } else {
         dzn = fminf(fabsf(dzn), hmn);
@@ -725,21 +733,24 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     if (own) {
       const long long gi = fx_ix(d, irow, icol);
       const float etapre = d.eta[pprev + gi];
-      float eta1 = etapre;
+      float eta1 = etapre, lo1 = d.eta_lo[pprev + gi];
       const uint8_t fl = d.flags[sprev + gi];
       const float hpre = fmaxf(0.0f, etapre);
-      uint8_t ld = (double)hpre > d.hdry ? 0 : 1;
+      uint8_t ld = fx_dd_val(etapre, lo1) > d.hdry ? 0 : 1;
       float h1 = hpre;
+      double depth = fx_dd_val(etapre, lo1);
       if (melt_on && !(fl & FX_F_NODATA)) {
         const double mi = melt_depth(d, c, gi);
         bmelt = mi * d.arbase;
         if (d.ade) d.hpm_f[scur + gi] = hpre;
-        eta1 = etapre + (float)mi;
+        fx_dd_add(eta1, lo1, (float)mi);
         h1 = fmaxf(eta1, 0.0f);
-        if ((double)h1 <= d.hdry) ld = 0;
+        depth = fx_dd_val(eta1, lo1);
+        if (depth <= d.hdry) ld = 0;
       }
       const float qx = d.qx_f[pprev + gi], qy = d.qy_f[pprev + gi];
       d.eta[pcur + gi] = eta1;
+      d.eta_lo[pcur + gi] = lo1;
       d.qx_f[pcur + gi] = qx;
       d.qy_f[pcur + gi] = qy;
       d.h_f[scur + gi] = h1;
@@ -749,7 +760,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         d.fe1_f[scur + gi] = d.fe1_f[sprev + gi];
         d.fn1_f[scur + gi] = d.fn1_f[sprev + gi];
       }
-      courant_cell(d, (double)h1, (double)qx, (double)qy, dtc, hm);
+      courant_cell(d, fmax(0.0, depth), (double)qx, (double)qy, dtc, hm);
     }
     reduce_courant(d, S, dtc, hm);
     reduce_budget(d, S.budget, bmelt, 0.0);
@@ -764,11 +775,12 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
   for (int k = tid; k < NSTEN; k += NTHREADS) {
     const int sr = k % SX, scc = k / SX;
     const int r = irow0 - 2 + sr, q = icol0 - 2 + scc;
-    float eta = 0.f, sx = 0.f, sy = 0.f, qx = 0.f, qy = 0.f;
+    float eta = 0.f, lo = 0.f, sx = 0.f, sy = 0.f, qx = 0.f, qy = 0.f;
     unsigned char cl = 0;
     if (r >= 0 && r <= d.nr + 1 && q >= 0 && q <= d.nc + 1) {
       const long long gi = fx_ix(d, r, q);
       eta = d.eta[pprev + gi];
+      lo = d.eta_lo[pprev + gi];
       sx = d.sx[gi];
       sy = d.sy[gi];
       qx = d.qx_f[pprev + gi];
@@ -777,8 +789,8 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         cl = C_INT;
         const uint8_t fl = d.flags[sprev + gi];
         if (fl & FX_F_WALL) cl |= C_WALL;
-        if (melt_on && !(fl & FX_F_NODATA)) eta = eta + (float)melt_depth(d, c, gi);
-        if ((double)fmaxf(0.0f, eta) <= d.hdry) {
+        if (melt_on && !(fl & FX_F_NODATA)) fx_dd_add(eta, lo, (float)melt_depth(d, c, gi));
+        if (fx_dd_val(eta, lo) <= d.hdry) {
           qx = 0.f;
           qy = 0.f;
           cl |= C_DRY;
@@ -786,6 +798,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       }
     }
     S.eta[k] = eta;
+    S.eta_lo[k] = lo;
     S.sx[k] = sx;
     S.sy[k] = sy;
     S.qx[k] = qx;
@@ -868,11 +881,13 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     const unsigned char clW = S.cls[sidx(lx + 1, ly + 2)], clS = S.cls[sidx(lx + 2, ly + 1)];
     const float qxfW = ((clW & C_INT) && !(clW & C_WALL)) ? S.f[0][fW] * dtl : 0.0f;
     const float qyfS = ((clS & C_INT) && !(clS & C_WALL)) ? S.f[3][fS] * dtl : 0.0f;
-    const float eta = eta1 + dh;
+    float eta = eta1, lo = S.eta_lo[sP];
+    fx_dd_add(eta, lo, dh);
     const float h = fmaxf(0.0f, eta);
+    const double depth = fx_dd_val(eta, lo);
     float qx, qy;
     uint8_t ld;
-    if ((double)h < d.hdry || wall) {
+    if (depth < d.hdry || wall) {
       qx = qy = 0.0f;
       ld = 1;
     } else {
@@ -892,6 +907,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       }
     }
     d.eta[pcur + gi] = eta;
+    d.eta_lo[pcur + gi] = lo;
     d.h_f[scur + gi] = h;
     d.qx_f[pcur + gi] = qx;
     d.qy_f[pcur + gi] = qy;
@@ -903,7 +919,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
                              (S.cls[sidx(lx + 2, ly + 1)] & C_DRY) && (S.cls[sidx(lx + 2, ly + 3)] & C_DRY));
       d.fe1_f[scur + gi] = S.f[0][fP];
       d.fn1_f[scur + gi] = S.f[3][fP];
-      if (computed && (d.store_all_fluxes || !((double)h > d.hdry))) {
+      if (computed && (d.store_all_fluxes || !(depth > d.hdry))) {
         d.fe2_f[gi] = S.f[1][fP];
         d.fe3_f[gi] = S.f[2][fP];
         d.fn2_f[gi] = S.f[4][fP];
@@ -913,7 +929,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       d.fe1_f[scur + gi] = 0.0f;
       d.fn1_f[scur + gi] = 0.0f;
     }
-    courant_cell(d, (double)h, (double)qx, (double)qy, dtc, hm);
+    courant_cell(d, fmax(0.0, depth), (double)qx, (double)qy, dtc, hm);
   }
   reduce_courant(d, S, dtc, hm);
   reduce_budget(d, S.budget, bmelt, bout);
@@ -1253,7 +1269,8 @@ __global__ void __launch_bounds__(BX * BY) k_courant_scan(const fx_dev* __restri
     const long long gi = fx_ix(d, irow, icol);
     const long long sl = fx_slot(d, d.ctl->steps), pl = fx_pp(d, d.ctl->steps);
     if (d.prec32)
-      courant_cell(d, (double)d.h_f[sl + gi], (double)d.qx_f[pl + gi], (double)d.qy_f[pl + gi], dtc, hm);
+      courant_cell(d, fmax(0.0, fx_dd_val(d.eta[pl + gi], d.eta_lo[pl + gi])), (double)d.qx_f[pl + gi],
+                   (double)d.qy_f[pl + gi], dtc, hm);
     else
       courant_cell(d, d.h[sl + gi], d.qx[pl + gi], d.qy[pl + gi], dtc, hm);
   }
@@ -1342,12 +1359,17 @@ __global__ void k_mark_static(const fx_dev* __restrict__ devs, int dom) {
   }
 }
 
-// FP32 state: eta = z - zb over the whole grid (ghost ring included), from a
-// staged FP64 z in the field layout, into both planes of eta.
+// FP32 state: the compensated depth (eta, eta_lo) = z - zb over the whole
+// grid (ghost ring included), from a staged FP64 z in the field layout, into
+// both planes.
 __global__ void k_eta_from_z(const __grid_constant__ fx_dev d, const double* __restrict__ z) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < d.plane;
-       i += (long long)gridDim.x * blockDim.x)
-    d.eta[i] = d.eta[d.plane + i] = (float)(z[i] - d.zb[i]);
+       i += (long long)gridDim.x * blockDim.x) {
+    const double depth = z[i] - d.zb[i];
+    const float hi = (float)depth;
+    d.eta[i] = d.eta[d.plane + i] = hi;
+    d.eta_lo[i] = d.eta_lo[d.plane + i] = (float)(depth - (double)hi);
+  }
 }
 
 // FP32 state: the bed differences to the east and north neighbours of every
@@ -1382,7 +1404,7 @@ __global__ void __launch_bounds__(256) k_mass(const __grid_constant__ fx_dev d, 
     if (irow < 1 || irow > d.nr || icol < 1 || icol > d.nc) continue;
     if (d.flags[sl + i] & FX_F_WALL) continue;
     const double h = d.prec32 ? (double)d.h_f[sl + i] : d.h[sl + i];
-    acc[0] += d.prec32 ? (double)d.eta[pl + i] : d.z[pl + i] - d.zb[i];
+    acc[0] += d.prec32 ? fx_dd_val(d.eta[pl + i], d.eta_lo[pl + i]) : d.z[pl + i] - d.zb[i];
     for (int k = 0; k < d.nchem; ++k)
       acc[1 + k] += h * (d.prec32 ? (double)d.conc_f[k * d.plane + i] : d.conc[k * d.plane + i]);
   }
