@@ -46,15 +46,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s FP32 vs FP64 at stated depth/mass error; p50/p99 request latency"
-# Algorithmic bytes per cell-update, per kernel (read + write of the flow
-# state, read of the bed, wall flag, Manning n and melt field; read + write of
-# the solute):
-#   FP64: hydro 2*8*3 (h or z, qx, qy) + 8 (zb) + 1 + 8 (n) + 8 (melt) = 73 B,
-#         ADE 2*8 = 16 B, step 89 B;
-#   FP32: hydro 2*4*3 (eta, qx, qy) + 8 (bed differences sx, sy) + 1 + 4 + 4
-#         = 41 B, ADE 2*4 = 8 B, step 49 B.
+# Algorithmic bytes per cell-update, per kernel: read + write of the flow
+# state and the solute, read of the bed, wall flag, Manning n and melt field
+# (B = 2w(3+ns) + w_zb + 1 + w_n + 4 with ns = 1):
+#   FP64: hydro 2*8*3 (z, qx, qy) + 8 (zb) + 1 + 8 (n) + 8 (melt, stored as
+#         FP64 here) = 73 B, ADE 2*8 = 16 B, step 89 B;
+#   FP32: hydro 2*4*3 + 4 + 1 + 4 + 4 = 37 B, ADE 2*4 = 8 B, step 45 B.
+# The FP32 layout moves more than that (the depth's compensation word and an
+# FP64 bed: 49 B of hydro state); the roofline's `traffic` field gives what
+# the kernel actually moved.
 ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
-             "fp32": {"k_hydro": 41, "k_ade_sweep": 8, "step": 49}}
+             "fp32": {"k_hydro": 37, "k_ade_sweep": 8, "step": 45}}
 
 
 def _rank():
@@ -152,10 +154,12 @@ def build_domain(sc, in_flight: int = 8, precision: str = "fp64"):
     return S.make_domain(sc, precision=precision, steps_in_flight=in_flight)
 
 
-def e2e_run(d, sc, steps: int):
+def e2e_run(d, sc, steps: int, chunk: int):
     """Through the public API with host buffers: upload the state from
-    pinned host memory, step (each step reads its status back), download the
-    Results fields. Returns (seconds, h2d bytes, d2h bytes)."""
+    pinned host memory, step in calls of `chunk` steps (the steps whose ADE
+    sweeps run in one launch; every call reads back the control block, which
+    holds each of its steps' dt and clock record), download the Results
+    fields. Returns (seconds, h2d bytes, d2h bytes)."""
     import torch
     shape = d.shape
     names_up = ("z", "h", "qx", "qy", "conc", "twet")
@@ -175,15 +179,36 @@ def e2e_run(d, sc, steps: int):
         d.upload(k, host[k])
     d.upload_flags(ldry, wall)
     d.prepare()
-    for _ in range(steps):
-        d.step(1)
+    left, calls = steps, 0
+    while left > 0:
+        n = min(chunk, left)
+        d.step(n)
+        left -= n
+        calls += 1
     for k in names_dn:
         d.download(k, out[k])
     t1 = time.perf_counter()
     cells = shape[0] * shape[1]
-    h2d = cells * (8 * len(names_up) + 8) + 8 * steps
-    d2h = cells * 8 * len(names_dn) + 256 * steps
+    h2d = cells * (8 * len(names_up) + 8) + 8 * calls
+    d2h = cells * 8 * len(names_dn) + 1600 * calls
     return t1 - t0, h2d, d2h
+
+
+class _stdout_to_stderr:
+    """The reference's start-up prints progress to stdout (fd 1); keep the
+    one JSON line of this program alone there."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
 
 
 def cpu_reference_run(sc, h, conc, warmup: int, steps: int, crop: int):
@@ -198,7 +223,7 @@ def cpu_reference_run(sc, h, conc, warmup: int, steps: int, crop: int):
     sub = S.Scenario(name=f"crop{n}", dem=sc.dem[:n, :n].copy(), dxy=sc.dxy,
                      meteo=sc.meteo, horizon=sc.horizon, print_step=sc.print_step, ks=sc.ks,
                      ade=True, d_coef=sc.d_coef)
-    with tempfile.TemporaryDirectory() as tmp:
+    with tempfile.TemporaryDirectory() as tmp, _stdout_to_stderr():
         mp = sub.write(tmp)
         ref = P.RefRun(mp, sub, 0)
         ref.apply_wet_start(h[:n, :n], None, None, [conc[:n, :n]])
@@ -275,11 +300,13 @@ def run_mix(args, peak: float) -> dict:
     steps = args.mix_steps
 
     def batch_rate(precision):
-        doms = [S.make_domain(sc, precision=precision, steps_in_flight=8) for sc in scs]
+        doms = [S.make_domain(sc, precision=precision, steps_in_flight=args.in_flight) for sc in scs]
         b = fx.Batch()
         for d in doms:
             b.add(d)
-        tuned = b.autotune(4) if precision == "fp32" else (8, 8)
+        tuned = b.autotune(4) if precision == "fp32" else (8, args.in_flight)
+        if precision == "fp64":
+            b.set_option("steps_in_flight", args.in_flight)
         b.step(args.warmup)
         s0 = [d.status()["steps"] for d in doms]
         stream = torch.cuda.ExternalStream(b.stream())
@@ -302,7 +329,7 @@ def run_mix(args, peak: float) -> dict:
     # plain FP64 path: each scenario alone, one after another
     tot_ms, tot_cells = 0.0, 0
     for sc, c in zip(scs, cells):
-        d = S.make_domain(sc, precision="fp64", steps_in_flight=8)
+        d = S.make_domain(sc, precision="fp64", steps_in_flight=args.in_flight)
         d.step(args.warmup)
         s0 = d.status()["steps"]
         ms, _, _ = d.time_steps(steps)
@@ -378,11 +405,12 @@ def run_gpu(args):
         acc = accuracy_of(doms["fp32"], doms["fp64"], w0["fp32"], w0["fp64"], sc.ks)
     e2e = None
     if not args.no_e2e:
-        secs, h2d, d2h = e2e_run(doms[head], sc, args.steps)
+        secs, h2d, d2h = e2e_run(doms[head], sc, args.steps, k_batch)
         e2e = {"value": cells * args.steps / secs, "unit": "cell-updates/s",
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
-               "note": "upload of the state from pinned host memory, K steps each reading its "
-                       "status back, download of the Results fields; per-step bytes = totals / K"}
+               "note": "upload of the state from pinned host memory, the K steps through fx_step in "
+                       "calls of steps-in-flight steps (each call reads the control block with every "
+                       "step's record back), download of the Results fields; per-step bytes = totals / K"}
     for d in doms.values():
         d.close()
     batches = (args.steps + k_batch - 1) // k_batch
@@ -457,15 +485,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-crop", type=int, default=2048)
     ap.add_argument("--cpu-steps", type=int, default=12)
-    ap.add_argument("--in-flight", type=int, default=8, help="steps per ADE launch (1..15)")
+    ap.add_argument("--in-flight", type=int, default=31, help="steps per ADE launch (1..31)")
     ap.add_argument("--precision", default="both", choices=("both", "fp64", "fp32"),
                     help="both: FP32 headline with FP64 beside it and the FP32 error")
     ap.add_argument("--no-mix", action="store_true")
     ap.add_argument("--mix-count", type=int, default=64)
-    ap.add_argument("--mix-steps", type=int, default=24)
+    ap.add_argument("--mix-steps", type=int, default=62)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
-    ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 720.0)
+    ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 120.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -248,7 +248,7 @@ int fx_batch_set_option(fx_batch* b, const char* name, long long v) {
     if (!fx_tile_rows_ok((int)v)) return fx_fail(nullptr, FX_ERR_ARG, "tile_rows must be 4, 8 or 16");
     b->tile_rows = (int)v;
   } else if (!strcmp(name, "steps_in_flight")) {
-    if (v < 1 || v > FX_MAX_SLOTS - 1) return fx_fail(nullptr, FX_ERR_ARG, "steps_in_flight must be 1..15");
+    if (v < 1 || v > FX_MAX_SLOTS - 1) return fx_fail(nullptr, FX_ERR_ARG, "steps_in_flight must be 1..31");
     b->k_limit = (int)v;
   } else {
     return fx_fail(nullptr, FX_ERR_ARG, "fx_batch_set_option: unknown option '%s'", name);
@@ -299,7 +299,7 @@ int fx_batch_autotune(fx_batch* b, int trial_steps, int* tile_rows, int* steps_i
   b->dirty = true;
   int best_k = std::min(b->k_limit, kmax);
   best = -1;
-  for (int k : {2, 4, 8, 15}) {
+  for (int k : {2, 4, 8, 16, 31}) {
     if (k > kmax) continue;
     b->k_limit = k;
     b->dirty = true;

@@ -213,7 +213,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
     if ((rc = dev_alloc(c, (void**)&d.conc, pb * g->nchem)) != FX_OK) goto fail;
   } else {
     const size_t pf = (size_t)d.plane * sizeof(float);
-    float** fields[] = {&d.sx, &d.sy, &d.twet_f, &d.fe2_f, &d.fe3_f, &d.fn2_f, &d.fn3_f};
+    float** fields[] = {&d.twet_f, &d.fe2_f, &d.fe3_f, &d.fn2_f, &d.fn3_f};
     float** pair_fields[] = {&d.eta, &d.eta_lo, &d.qx_f, &d.qy_f};
     float** slot_fields[] = {&d.h_f, &d.h0_f, &d.hpm_f, &d.fe1_f, &d.fn1_f};
     if ((rc = dev_alloc(c, (void**)&d.zb, (size_t)d.plane * sizeof(double))) != FX_OK) goto fail;
@@ -320,7 +320,7 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
   const long long gx = (g->nrows + 30) / 31, gy = (g->ncols + 6) / 7;
   long long b = 0;
   if (p->precision == 1)
-    b += plane * (8 + 7 * 4 + 4 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids);
+    b += plane * (8 + 5 * 4 + 4 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids);
   else
     b += plane * (6 * 8 + 3 * 2 * 8 + 5 * 8 * nslot + 8LL * g->nchem + 8LL * extension_grids);
   b += plane * nslot;                                   // flags
@@ -402,8 +402,25 @@ int fx_upload(fx_ctx* c, const char* field, const double* host) {
     if ((rc = put_grid(c, c->d.zb, false, 1, host))) return rc;
   } else {
     const FieldRef f = field_ref(c, field);
-    // every slot (and both planes of a pair) holds the uploaded state
-    if ((rc = put_grid(c, f.ptr, f.f32, f.slot ? c->d.nslot : (f.pair ? 2 : 1), host))) return rc;
+    // Every plane of a slot or pair field holds the uploaded grid: the steps
+    // overwrite the interior cells only, and the ghost ring they read stays
+    // as uploaded. The host grid crosses PCIe once, into the current plane;
+    // the other planes are device-to-device copies of it.
+    const size_t esz = f.f32 ? sizeof(float) : sizeof(double);
+    const int planes = f.slot ? c->d.nslot : (f.pair ? 2 : 1);
+    long long cur = 0;
+    if (planes > 1) {
+      if ((rc = read_ctl(c))) return rc;
+      cur = f.slot ? c->ctl_host->steps % c->d.nslot : (c->ctl_host->steps & 1);
+    }
+    char* base = (char*)f.ptr;
+    const size_t pbytes = (size_t)c->d.plane * esz;
+    if ((rc = put_grid(c, base + cur * pbytes, f.f32, 1, host))) return rc;
+    for (int k = 0; k < planes; ++k)
+      if (k != cur)
+        FX_CK(c, cudaMemcpyAsync(base + k * pbytes, base + cur * pbytes, pbytes, cudaMemcpyDeviceToDevice,
+                                 c->stream));
+    FX_CK(c, cudaStreamSynchronize(c->stream));
   }
   c->prepared = false;
   return FX_OK;
@@ -552,7 +569,6 @@ int fx_prepare(fx_ctx* c) {
       if (r2) return r2;
       c->z_pending.clear();
     }
-    fx_launch_bed_slopes(c->d, c->stream);
   }
   fx_launch_mark_static(c->d_dev, 0, c->stream);
   fx_launch_courant_scan(c->d_dev, c->d_tiles, c->ntiles, c->d.tile_rows, c->stream);

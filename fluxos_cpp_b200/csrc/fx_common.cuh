@@ -14,7 +14,7 @@
 #define FX_ROFF 1
 #define FX_MAX_CHEM 8
 #define FX_METEO_ROWS 2000
-#define FX_MAX_SLOTS 16
+#define FX_MAX_SLOTS 32
 
 // Per-cell flag byte.
 #define FX_F_LDRY 0x01       // ldry (1 = dry) at the end of the last step
@@ -122,15 +122,15 @@ struct fx_dev {
   // Single-precision state (prec32 = 1, fx_hydro.cu hydro_tile32): the depth
   // above the bed eta = z - zb is stored, and the bed enters only through
   // its differences to the east and north neighbours (sx = zb(E) - zb(P),
-  // sy = zb(N) - zb(P)), so water-surface differences are sx + (eta_E -
-  // eta_P) and thin films keep their digits. The depth is held compensated,
+  // sy = zb(N) - zb(P), exact in FP64 from the FP64 bed), so water-surface
+  // differences are sx + (eta_E - eta_P) and thin films keep their digits. The depth is held compensated,
   // as the pair (eta, eta_lo) with eta + eta_lo exact and |eta_lo| at most
   // half an ulp of eta: flux arithmetic reads eta alone, updates add to the
   // pair without rounding loss, and the wet/dry threshold tests compare
   // eta + eta_lo in FP64. zb stays FP64 for output.
   int prec32;
   int pad4_;
-  float *eta, *eta_lo, *sx, *sy, *qx_f, *qy_f, *twet_f;
+  float *eta, *eta_lo, *qx_f, *qy_f, *twet_f;
   float *h_f, *h0_f, *hpm_f, *fe1_f, *fn1_f;  // nslot planes each
   float *fe2_f, *fe3_f, *fn2_f, *fn3_f;
   float* conc_f;                              // nchem planes

@@ -473,8 +473,9 @@ __device__ __forceinline__ double melt_depth(const fx_dev& d, const StepCtl& c, 
 
 
 // ===================== single-precision step (prec32) =======================
-// The same step as k_hydro's FP64 body, on the depth eta = z - zb and the bed
-// differences sx, sy (fx_common.cuh): every water-surface difference of the
+// The same step as the FP64 body, on the depth eta = z - zb and the bed
+// differences sx = zb(E) - zb(P), sy = zb(N) - zb(P), formed exactly in FP64
+// from the stencil's bed values: every water-surface difference of the
 // reference is rewritten without the bed elevation itself,
 //   ze - zp = sx(P) + (eta_E - eta_P),  zp - zbpe = eta_P - sx(P)/2,
 //   ze - zbpe = eta_E + sx(P)/2,        h = max(0, eta),
@@ -489,7 +490,8 @@ struct HydroSmem32 {
   static constexpr int NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX, NW = Tile<BY>::NTHREADS / 32;
   double budget[2 * NW];
   double red_dt[NW], red_h[NW];
-  float eta[NSTEN], eta_lo[NSTEN], sx[NSTEN], sy[NSTEN], qx[NSTEN], qy[NSTEN];
+  double zb[NSTEN];
+  float eta[NSTEN], eta_lo[NSTEN], qx[NSTEN], qy[NSTEN];
   float f[6][NFLUX];
   unsigned char cls[NSTEN];
   short wet_list[NFLUX], dry_list[NFLUX], stale_list[NFLUX];
@@ -516,7 +518,9 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   bool lroe = true;
   float volrat = d.volrat_mode == 0 ? __int_as_float(0x7f800000) : 0.0f;
   const bool ldp_dry = S.cls[P] & C_DRY, lde_dry = S.cls[E] & C_DRY, ldn_dry = S.cls[N] & C_DRY;
-  const float etap = S.eta[P], sxp = S.sx[P], syp = S.sy[P];
+  // bed differences: exact in FP64 for the branch tests, rounded for the flux arithmetic
+  const double sx_d = S.zb[E] - S.zb[P], sy_d = S.zb[N] - S.zb[P];
+  const float etap = S.eta[P], sxp = (float)sx_d, syp = (float)sy_d;
   // compensated depths for the branch tests (FP64, as the FP64 path decides them)
   const double dP = fx_dd_val(etap, S.eta_lo[P]), dE = fx_dd_val(S.eta[E], S.eta_lo[E]);
   const double dN = fx_dd_val(S.eta[N], S.eta_lo[N]);
@@ -537,11 +541,12 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   if (lde_dry) {
     hme = fmaxf(0.0f, etap - .5f * sxp);
     he = qe = re = 0.0f;
-    if (fmax(0.0, dP - .5 * (double)sxp) > hdry) {
-      if ((double)sxp + (dE - dP) >= 0.0) {
+    const double dze_d = sx_d + (dE - dP);
+    if (fmax(0.0, dP - .5 * sx_d) > hdry) {
+      if (dze_d >= 0.0) {
         qme = rme = 0.0f;
       } else {
-        dze = fminf(fabsf(dze), hme);
+        dze = fminf((float)fabs(dze_d), hme);
         qme = 0.296f * dze * sqrtf(gaccl * dze);
         volrat = 0.5f * dx * hp / dtl;
         qme = fminf(qme, volrat);
@@ -555,11 +560,12 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   if (ldn_dry) {
     hmn = fmaxf(0.0f, etap - .5f * syp);
     hn = qn = rn = 0.0f;
-    if (fmax(0.0, dP - .5 * (double)syp) > hdry) {
-      if ((double)syp + (dN - dP) >= 0.0) {
+    const double dzn_d = sy_d + (dN - dP);
+    if (fmax(0.0, dP - .5 * sy_d) > hdry) {
+      if (dzn_d >= 0.0) {
         qmn = rmn = 0.0f;
       } else {
-        dzn = fminf(fabsf(dzn), hmn);
+        dzn = fminf((float)fabs(dzn_d), hmn);
         rmn = 0.296f * dzn * sqrtf(gaccl * dzn);
         qmn = 0.0f;
         volrat = 0.5f * dy * hp / dtl;
@@ -664,7 +670,8 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
   const float gaccl = (float)d.gaccl;
   float volrat = d.volrat_mode == 0 ? __int_as_float(0x7f800000) : 0.0f;
   const bool lde_dry = S.cls[E] & C_DRY, ldn_dry = S.cls[N] & C_DRY;
-  const float etap = S.eta[P], etae = S.eta[E], etan = S.eta[N], sxp = S.sx[P], syp = S.sy[P];
+  const double sx_d = S.zb[E] - S.zb[P], sy_d = S.zb[N] - S.zb[P];
+  const float etap = S.eta[P], etae = S.eta[E], etan = S.eta[N], sxp = (float)sx_d, syp = (float)sy_d;
   const double dP = fx_dd_val(etap, S.eta_lo[P]), dE = fx_dd_val(etae, S.eta_lo[E]);
   const double dN = fx_dd_val(etan, S.eta_lo[N]);
   const float he = fmaxf(0.0f, etae), hn = fmaxf(0.0f, etan);
@@ -672,33 +679,41 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
   float fe1 = 0.f, fe2 = 0.f, fe3 = 0.f, fn1 = 0.f, fn2 = 0.f, fn3 = 0.f;
   if (!lde_dry) {
     float hme = fmaxf(0.0f, etae + .5f * sxp);
-    if (fmax(0.0, dE + .5 * (double)sxp) > d.hdry) {
-      if ((double)sxp + (dE - dP) <= 0.0) {
+    const double dze_d = sx_d + (dE - dP);
+    if (fmax(0.0, dE + .5 * sx_d) > d.hdry) {
+      if (dze_d <= 0.0) {
         fe2 = .5f * gaccl * hme * hme;
       } else {
-        dze = fminf(fabsf(dze), hme);
-        float qme = 0.296f * dze * sqrtf(gaccl * dze);
-        hme = 0.444f * dze;
+        // the surface difference is positive (decided in FP64); its FP32
+        // value can round to 0, where the inflow and its momentum are 0
+        dze = fminf((float)dze_d, hme);
         volrat = (float)d.dxy * he / dtl;
-        qme = -fminf(qme, volrat);
-        fe1 = qme;
-        fe2 = qme * (qme / hme) + .5f * gaccl * hme * hme;
+        if (dze > 0.0f) {
+          float qme = 0.296f * dze * sqrtf(gaccl * dze);
+          hme = 0.444f * dze;
+          qme = -fminf(qme, volrat);
+          fe1 = qme;
+          fe2 = qme * (qme / hme) + .5f * gaccl * hme * hme;
+        }
       }
     }
   }
   if (!ldn_dry) {
     float hmn = fmaxf(0.0f, etan + .5f * syp);
-    if (fmax(0.0, dN + .5 * (double)syp) > d.hdry) {
-      if ((double)syp + (dN - dP) <= 0.0) {
+    const double dzn_d = sy_d + (dN - dP);
+    if (fmax(0.0, dN + .5 * sy_d) > d.hdry) {
+      if (dzn_d <= 0.0) {
         fn3 = .5f * gaccl * hmn * hmn;
       } else {
-        dzn = fminf(fabsf(dzn), hmn);
-        float rmn = 0.296f * dzn * sqrtf(gaccl * dzn);
-        hmn = 0.444f * dzn;
+        dzn = fminf((float)dzn_d, hmn);
         volrat = (float)d.dxy * hn / dtl;
-        rmn = -fminf(rmn, volrat);
-        fn1 = rmn;
-        fn3 = rmn * (rmn / hmn) + .5f * gaccl * hmn * hmn;
+        if (dzn > 0.0f) {
+          float rmn = 0.296f * dzn * sqrtf(gaccl * dzn);
+          hmn = 0.444f * dzn;
+          rmn = -fminf(rmn, volrat);
+          fn1 = rmn;
+          fn3 = rmn * (rmn / hmn) + .5f * gaccl * hmn * hmn;
+        }
       }
     }
   }
@@ -775,14 +790,14 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
   for (int k = tid; k < NSTEN; k += NTHREADS) {
     const int sr = k % SX, scc = k / SX;
     const int r = irow0 - 2 + sr, q = icol0 - 2 + scc;
-    float eta = 0.f, lo = 0.f, sx = 0.f, sy = 0.f, qx = 0.f, qy = 0.f;
+    float eta = 0.f, lo = 0.f, qx = 0.f, qy = 0.f;
+    double zb = 0.0;
     unsigned char cl = 0;
     if (r >= 0 && r <= d.nr + 1 && q >= 0 && q <= d.nc + 1) {
       const long long gi = fx_ix(d, r, q);
       eta = d.eta[pprev + gi];
       lo = d.eta_lo[pprev + gi];
-      sx = d.sx[gi];
-      sy = d.sy[gi];
+      zb = d.zb[gi];
       qx = d.qx_f[pprev + gi];
       qy = d.qy_f[pprev + gi];
       if (r >= 1 && r <= d.nr && q >= 1 && q <= d.nc) {
@@ -799,8 +814,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     }
     S.eta[k] = eta;
     S.eta_lo[k] = lo;
-    S.sx[k] = sx;
-    S.sy[k] = sy;
+    S.zb[k] = zb;
     S.qx[k] = qx;
     S.qy[k] = qy;
     S.cls[k] = cl;
@@ -1216,15 +1230,15 @@ __device__ __forceinline__ void hydro_block(const fx_dev& d, const fx_tile& tile
   else hydro_tile64<BY>(d, c, tile, S);
 }
 
-// Blocks per SM the launch bounds ask for: 512 threads, at most 128
-// registers each.
-template <int BY>
-constexpr int min_blocks() { return 16 / BY; }
+// Blocks per SM the launch bounds ask for: 512 threads for FP64 (at most 128
+// registers each), 768 for FP32 (at most 85).
+template <bool P32, int BY>
+constexpr int min_blocks() { return (P32 ? 24 : 16) / BY > 0 ? (P32 ? 24 : 16) / BY : 1; }
 
 // One domain: the descriptor is a kernel parameter (constant bank), so its
 // fields are instruction operands. Block (x, y) is tile (x, y).
 template <bool P32, int BY>
-__global__ void __launch_bounds__(BX * BY, min_blocks<BY>()) k_hydro_one(const __grid_constant__ fx_dev d) {
+__global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>()) k_hydro_one(const __grid_constant__ fx_dev d) {
   __shared__ HydroSmem<BY> S;
   __shared__ StepCtl sc;
   const fx_tile tile{0, (int)blockIdx.x, (int)blockIdx.y, 0};
@@ -1234,7 +1248,7 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<BY>()) k_hydro_one(const _
 // A batch of domains: one block per entry of the tile table; the block copies
 // its domain's descriptor to shared memory.
 template <bool P32, int BY>
-__global__ void __launch_bounds__(BX * BY, min_blocks<BY>()) k_hydro_batch(const fx_dev* __restrict__ devs,
+__global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>()) k_hydro_batch(const fx_dev* __restrict__ devs,
                                                                         const fx_tile* __restrict__ tiles) {
   __shared__ HydroSmem<BY> S;
   __shared__ fx_dev sd;
@@ -1372,22 +1386,6 @@ __global__ void k_eta_from_z(const __grid_constant__ fx_dev d, const double* __r
   }
 }
 
-// FP32 state: the bed differences to the east and north neighbours of every
-// interior cell, rounded once from FP64 (0 on the ghost ring).
-__global__ void k_bed_slopes(const __grid_constant__ fx_dev d) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < d.plane;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int icol = (int)(i / d.ld), irow = (int)(i % d.ld) - FX_ROFF;
-    float sx = 0.0f, sy = 0.0f;
-    if (irow >= 1 && irow <= d.nr && icol >= 1 && icol <= d.nc) {
-      sx = (float)(d.zb[i + 1] - d.zb[i]);
-      sy = (float)(d.zb[i + d.ld] - d.zb[i]);
-    }
-    d.sx[i] = sx;
-    d.sy[i] = sy;
-  }
-}
-
 // Stored water sum(z - zb) * dxy^2 over the interior cells that are not
 // walls (the quantity the update conserves: a cell overdrawn by its
 // neighbours' outflow holds a small negative depth until it refills, where h
@@ -1470,7 +1468,6 @@ void fx_launch_courant_scan(const fx_dev* devs, const fx_tile* tiles, int ntiles
 void fx_launch_eta_from_z(const fx_dev& d, const double* z, cudaStream_t s) {
   fx::k_eta_from_z<<<592, 256, 0, s>>>(d, z);
 }
-void fx_launch_bed_slopes(const fx_dev& d, cudaStream_t s) { fx::k_bed_slopes<<<592, 256, 0, s>>>(d); }
 void fx_launch_mass(const fx_dev& d, double* out, cudaStream_t s) { fx::k_mass<<<296, 256, 0, s>>>(d, out); }
 // Appends the tiles of domain `dom` (nr x nc interior cells) to a table.
 void fx_tiles_of(int dom, int nr, int nc, int tile_rows, std::vector<fx_tile>& out) {

@@ -58,7 +58,6 @@ void fx_launch_courant_scan(const fx_dev* devs, const fx_tile* tiles, int ntiles
 void fx_launch_ade(const fx_dev* devs, const fx_unit* units, int nunits, int nblocks, bool prec32, cudaStream_t s);
 void fx_launch_ade_one(const fx_dev& d, int nunits, int nblocks, cudaStream_t s);
 void fx_launch_eta_from_z(const fx_dev& d, const double* z, cudaStream_t s);
-void fx_launch_bed_slopes(const fx_dev& d, cudaStream_t s);
 void fx_launch_mass(const fx_dev& d, double* out, cudaStream_t s);
 void fx_tiles_of(int dom, int nr, int nc, int tile_rows, std::vector<fx_tile>& out);
 bool fx_tile_rows_ok(int tile_rows);

@@ -17,9 +17,9 @@ launches, each with its own clock and dt:
   between chunks, its result is taken and its memory freed, which makes room
   for the next arrivals.
 
-Scenario inputs (terrain and fields) are generated on host threads ahead of
-admission so the GPU does not wait for them. Latency of a request is the
-time from its arrival to its retirement.
+A request's preparation (input generation, context creation and upload) runs
+on a host thread once it has arrived, while the batch keeps stepping. Latency
+of a request is the time from its arrival to its retirement.
 """
 from __future__ import annotations
 
@@ -49,7 +49,7 @@ class Request:
     nchem: int = 1
     extension_grids: int = 2
     precision: str = "fp32"
-    steps_in_flight: int = 4
+    steps_in_flight: int = 8
     # filled in by the server
     admitted: Optional[float] = None
     done: Optional[float] = None
@@ -81,6 +81,7 @@ class Server:
         self.on_output = on_output
         self.clock = clock
         self.pool = cf.ThreadPoolExecutor(max_workers=host_threads)
+        self.lookahead = host_threads
         self.batch = fx.Batch()
         self.active: List[tuple] = []  # (request, domain, bytes)
         self.used = 0
@@ -113,41 +114,51 @@ class Server:
         self.used -= nbytes
         r.done = now
 
+    def _prepare(self, r: Request):
+        """Host thread: the request's inputs and its resident domain."""
+        sc = r.make()
+        return S.make_domain(sc, precision=r.precision, steps_in_flight=r.steps_in_flight)
+
     def run(self, requests: List[Request]) -> dict:
         """Serve `requests` (arrival times in seconds from the call) to the
-        end; returns throughput and latency figures."""
+        end; returns throughput and latency figures.
+
+        A request's preparation (input generation, device allocation and
+        upload on the request's own stream) starts when it has arrived and
+        its footprint fits under the cap beside the resident members and the
+        preparations in progress; it runs on a host thread while the batch
+        keeps stepping. Prepared requests join the batch between chunks."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
-        futures = {}
+        preparing = collections.OrderedDict()  # rid -> (request, future, reserved bytes)
+        reserved = 0
         t0 = self.clock()
-        lookahead = 8
-        while pending or self.active:
+        while pending or preparing or self.active:
             now = self.clock() - t0
-            # host-side input generation ahead of admission
-            for r in list(pending)[:lookahead]:
-                if r.rid not in futures:
-                    futures[r.rid] = self.pool.submit(r.make)
-            # admission in arrival order while the footprint fits
-            while pending and pending[0].arrival <= now:
+            # start preparations in arrival order while memory and threads allow
+            while pending and pending[0].arrival <= now and len(preparing) < self.lookahead:
                 r = pending[0]
                 need = self.footprint(r)
-                if self.active and self.used + need > self.cap:
+                if (self.active or preparing) and self.used + reserved + need > self.cap:
                     break
-                sc = futures.pop(r.rid).result()
-                d = S.make_domain(sc, precision=r.precision, steps_in_flight=r.steps_in_flight)
+                preparing[r.rid] = (r, self.pool.submit(self._prepare, r), need)
+                reserved += need
+                pending.popleft()
+            # admit finished preparations
+            for rid in [k for k, (_, f, _) in preparing.items() if f.done()]:
+                r, f, need = preparing.pop(rid)
+                reserved -= need
+                d = f.result()
                 self.batch.add(d)
                 nbytes = d.device_bytes()
                 self.active.append((r, d, nbytes))
                 self.used += nbytes
-                self.peak_used = max(self.peak_used, self.used)
+                self.peak_used = max(self.peak_used, self.used + reserved)
                 self.peak_members = max(self.peak_members, len(self.active))
                 r.admitted = self.clock() - t0
-                pending.popleft()
-                now = self.clock() - t0
             if not self.active:
-                if pending:
-                    time.sleep(max(0.0, min(0.002, pending[0].arrival - (self.clock() - t0))))
+                time.sleep(0.001)
                 continue
-            before = [st["steps"] for st in (d.status() for _, d, _ in self.active)]
+            before = [d.status()["steps"] for _, d, _ in self.active]
             g0 = self.clock()
             sts = self.batch.step(self.chunk)
             self.gpu_busy += self.clock() - g0
@@ -167,11 +178,14 @@ class Server:
                     self._retire(i, now)
         wall = self.clock() - t0
         lat = np.array([r.latency for r in requests if r.latency is not None])
+        wait = np.array([r.admitted - r.arrival for r in requests if r.admitted is not None])
         return {"requests": len(requests), "wall_s": wall,
                 "cell_updates": self.cell_updates,
                 "cell_updates_per_s": self.cell_updates / wall if wall > 0 else 0.0,
                 "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
                 "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
+                "admission_p50_s": float(np.percentile(wait, 50)) if wait.size else None,
+                "admission_p99_s": float(np.percentile(wait, 99)) if wait.size else None,
                 "peak_device_bytes": self.peak_used, "peak_members": self.peak_members,
                 "batch_step_s": self.gpu_busy}
 
