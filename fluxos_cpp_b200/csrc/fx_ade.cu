@@ -105,13 +105,33 @@ struct Fields<float> {
   static __device__ __forceinline__ float* conc(const fx_dev& d) { return d.conc_f; }
 };
 
+// Division and square root: IEEE-rounded in FP64 (bit parity with the
+// reference); in FP32 the approximate hardware reciprocal and square root
+// (PTX rcp.approx / sqrt.approx) refined by one Newton step with fused
+// multiply-adds, without the IEEE code paths.
+__device__ __forceinline__ double tdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float tdiv(float a, float b) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+  const float q = a * r;
+  return fmaf(fmaf(-b, q, a), r, q);
+}
+__device__ __forceinline__ double tsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float tsqrt(float a) {
+  float s, r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(s) : "f"(a));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(s));
+  const float t = fmaf(fmaf(-s, s, a), 0.5f * r, s);
+  return a > 0.0f ? t : s;
+}
+
 template <class T>
 __device__ __forceinline__ T div_dxy(const fx_dev& d, T x) {
-  return d.dxy_pow2 ? x * (T)d.inv_dxy : x / (T)d.dxy;
+  return d.dxy_pow2 ? x * (T)d.inv_dxy : tdiv(x, (T)d.dxy);
 }
 template <class T>
 __device__ __forceinline__ T div_area(const fx_dev& d, T x) {
-  return d.dxy_pow2 ? x * (T)d.inv_area : x / (T)d.arbase;
+  return d.dxy_pow2 ? x * (T)d.inv_area : tdiv(x, (T)d.arbase);
 }
 
 // The step a unit works on.
@@ -200,12 +220,12 @@ __device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, con
         const T mi = Fields<T>::mm(d)
                          ? (T)((double)S.meteo_rate * (double)R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
                          : (T)S.meteoi;
-        c = (c * hp + (mi * (T)S.mconc)) / (h0);
+        c = tdiv(c * hp + (mi * (T)S.mconc), h0);
       }
     }
     r.c = c;
     if (!S.sweep) r.b = c;
-    else if (r.ld == 0 && ldp == 0) r.b = c * h0 / r.h;
+    else if (r.ld == 0 && ldp == 0) r.b = tdiv(c * h0, r.h);
     else if (r.ld == 1) r.b = T(0);
     else r.b = c;
     r.qx = R.fe1[slot][lane];
@@ -245,7 +265,7 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, T D, T dt, bool last_r
   T fem, pfde, hnue, hne;
   if (ldE == 0) {  // :151-172
     hnue = fmax(hp * nt * he * nt, T(.0001));
-    hne = div_dxy<T>(d, sqrt(hnue) * T(2)) * dy * D;  // sigc = 0.5: /sigc is *2 exactly
+    hne = div_dxy<T>(d, tsqrt(hnue) * T(2)) * dy * D;  // sigc = 0.5: /sigc is *2 exactly
     pfde = -hne * (fe - fp);
     if (qxl > T(0)) {
       if (ldW == 0) fem = T(-.125) * fw + T(.75) * fp + T(.375) * fe;
@@ -264,7 +284,7 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, T D, T dt, bool last_r
   T pfe = pfce + pfde;
   if (pfe < T(0)) {  // :187-194
     if (ldE == 0) {
-      const T cvolrate = -(fe * he) * areae / dt;
+      const T cvolrate = tdiv(-(fe * he) * areae, dt);
       pfe = fmax(pfe, cvolrate);
     } else {
       pfe = T(0);
@@ -273,7 +293,7 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, T D, T dt, bool last_r
   T fnm, qfdn, hnn;
   if (ldN == 0) {  // :198-218
     hnue = fmax(T(.0001), hp * ntp * hn * nt);
-    hnn = div_dxy<T>(d, sqrt(hnue) * T(2)) * dx * D;
+    hnn = div_dxy<T>(d, tsqrt(hnue) * T(2)) * dx * D;
     qfdn = -hnn * (fn - fp);
     if (qyl > T(0)) {
       if (ldS == 0) fnm = T(-.125) * fs + T(.75) * fp + T(.375) * fn;
@@ -292,18 +312,18 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, T D, T dt, bool last_r
   T qfn = qfcn + qfdn;
   if (qfn < T(0)) {  // :234-241
     if (ldN == 0) {
-      const T cvolrate = -(fn * hn) * arean / dt;
+      const T cvolrate = tdiv(-(fn * hn) * arean, dt);
       qfn = fmax(qfn, cvolrate);
     } else {
       qfn = T(0);
     }
   }
   const T cvolpot = (fp * hp) * area;  // :243-278
-  const T cvolrat = cvolpot / dt + pfw + qfs;
+  const T cvolrat = tdiv(cvolpot, dt) + pfw + qfs;
   if (cvolrat > T(0)) {
     if (pfe > T(0) && qfn > T(0)) {
       if (pfe + qfn > cvolrat) {
-        const T cf = qfn / (pfe + qfn);
+        const T cf = tdiv(qfn, pfe + qfn);
         pfe = (T(1) - cf) * cvolrat;
         qfn = cf * cvolrat;
       }
@@ -327,7 +347,7 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, T D, T dt, bool last_r
     }
   }
   const T dc = div_area<T>(d, (pfw - pfe + qfs - qfn) * dt);  // :281-286
-  T cn = fp + dc / hp;
+  T cn = fp + tdiv(dc, hp);
   cn = fmin(cmax, cn);
   cn = fmax(cmin, cn);
   con = cn;
@@ -583,7 +603,8 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
 // One domain: the descriptor is a kernel parameter. Unit u is strip
 // u % nstrips of solute (u / nstrips) % nchem at step u / (nstrips * nchem).
 template <class T>
-__global__ void __launch_bounds__(WARPS * 32) k_ade_one(const __grid_constant__ fx_dev d, int nunits) {
+__global__ void __launch_bounds__(WARPS * 32, 3) k_ade_one(const __grid_constant__ fx_dev d,
+                                                                           int nunits) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -600,7 +621,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_ade_one(const __grid_constant__ 
 // A batch of domains: units come from the unit table; each warp copies its
 // unit's descriptor to its own shared-memory slot.
 template <class T>
-__global__ void __launch_bounds__(WARPS * 32) k_ade_batch(const fx_dev* __restrict__ devs,
+__global__ void __launch_bounds__(WARPS * 32, 3) k_ade_batch(const fx_dev* __restrict__ devs,
                                                          const fx_unit* __restrict__ units, int nunits) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ fx_dev wdev[WARPS];
@@ -658,6 +679,27 @@ static int max_blocks_of(K kernel, size_t smem, int nsm, int* out) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, fxade::WARPS * 32, smem) != cudaSuccess)
     return -1;
   *out = per * nsm;
+  return 0;
+}
+
+// Resident blocks of the sweep kernels of one precision on this device (the
+// smaller of the one-domain and batch forms), after raising their dynamic
+// shared memory limit.
+int fx_ade_max_blocks_for(bool prec32, int* out) {
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+  int a = 0, b = 0;
+  if (prec32) {
+    if (max_blocks_of(fxade::k_ade_one<float>, ade_smem(true), nsm, &a) ||
+        max_blocks_of(fxade::k_ade_batch<float>, ade_smem(true), nsm, &b))
+      return -1;
+  } else {
+    if (max_blocks_of(fxade::k_ade_one<double>, ade_smem(false), nsm, &a) ||
+        max_blocks_of(fxade::k_ade_batch<double>, ade_smem(false), nsm, &b))
+      return -1;
+  }
+  *out = std::min(a, b);
   return 0;
 }
 

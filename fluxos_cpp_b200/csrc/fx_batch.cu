@@ -107,7 +107,7 @@ static int rebuild(fx_batch* b) {
   b->ntiles = (int)tiles.size();
   b->nunits = (int)units.size();
   int maxb = 0;
-  if (fx_ade_max_blocks(&maxb) != 0 || maxb < 1) {
+  if (fx_ade_max_blocks_for(n > 0 && b->doms[0]->d.prec32 != 0, &maxb) != 0 || maxb < 1) {
     int r = fx_fail(nullptr, FX_ERR_CUDA, "occupancy query for the ADE sweep failed");
     b->err = fx_last_error(nullptr);
     return r;

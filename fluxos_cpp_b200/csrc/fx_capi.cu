@@ -244,7 +244,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
     goto fail;
   {
     int maxb = 0;
-    if (fx_ade_max_blocks(&maxb) != 0 || maxb < 1) {
+    if (fx_ade_max_blocks_for(d.prec32 != 0, &maxb) != 0 || maxb < 1) {
       rc = fx_fail(c, FX_ERR_CUDA, "occupancy query for the ADE sweep failed");
       goto fail;
     }

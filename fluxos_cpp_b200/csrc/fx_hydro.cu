@@ -498,8 +498,40 @@ struct HydroSmem32 {
   int nwet, ndry, nstale;
 };
 
+// FP32 arithmetic divides and takes square roots by the approximate hardware
+// reciprocal and square root (PTX rcp.approx / sqrt.approx) refined by one
+// Newton step with fused multiply-adds: close to correctly rounded for the
+// finite, normal operands of this scheme, without the IEEE code paths; the
+// FP64 path keeps IEEE-rounded operations for bit parity with the reference.
+__device__ __forceinline__ float frcp(float a) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return fmaf(fmaf(-a, r, 1.0f), r, r);
+}
+__device__ __forceinline__ float fdiv(float a, float b) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+  const float q = a * r;
+  return fmaf(fmaf(-b, q, a), r, q);
+}
+__device__ __forceinline__ float fsqrt(float a) {
+  float s, r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(s) : "f"(a));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(s));
+  const float t = fmaf(fmaf(-s, s, a), 0.5f * r, s);
+  return a > 0.0f ? t : s;
+}
+// Cube root of h > 0 as 2^(log2(h) / 3) (the friction term only).
+__device__ __forceinline__ float fcbrt(float h) {
+  float l, r;
+  asm("lg2.approx.f32 %0, %1;" : "=f"(l) : "f"(h));
+  l = l * (1.0f / 3.0f);
+  asm("ex2.approx.f32 %0, %1;" : "=f"(r) : "f"(l));
+  return r;
+}
+
 __device__ __forceinline__ float div_dxy_f(const fx_dev& d, float x) {
-  return d.dxy_pow2 ? x * (float)d.inv_dxy : x / (float)d.dxy;
+  return d.dxy_pow2 ? x * (float)d.inv_dxy : fdiv(x, (float)d.dxy);
 }
 
 template <class SM>
@@ -547,8 +579,8 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
         qme = rme = 0.0f;
       } else {
         dze = fminf((float)fabs(dze_d), hme);
-        qme = 0.296f * dze * sqrtf(gaccl * dze);
-        volrat = 0.5f * dx * hp / dtl;
+        qme = 0.296f * dze * fsqrt(gaccl * dze);
+        volrat = fdiv(0.5f * dx * hp, dtl);
         qme = fminf(qme, volrat);
         rme = 0.0f;
       }
@@ -566,9 +598,9 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
         qmn = rmn = 0.0f;
       } else {
         dzn = fminf((float)fabs(dzn_d), hmn);
-        rmn = 0.296f * dzn * sqrtf(gaccl * dzn);
+        rmn = 0.296f * dzn * fsqrt(gaccl * dzn);
         qmn = 0.0f;
-        volrat = 0.5f * dy * hp / dtl;
+        volrat = fdiv(0.5f * dy * hp, dtl);
         rmn = fminf(rmn, volrat);
       }
     } else {
@@ -576,21 +608,23 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
     }
     lroe = false;
   }
-  const float cme = sqrtf(gaccl * hme), cmn = sqrtf(gaccl * hmn);
-  const float ume = qme / fmaxf(hme, hdryl), vme = rme / fmaxf(hme, hdryl);
-  const float umn = qmn / fmaxf(hmn, hdryl), vmn = rmn / fmaxf(hmn, hdryl);
-  const float hne = nueml * sqrtf(hp * he);  // (cvdef*us*h + nuem), us = 0
-  const float hnn = nueml * sqrtf(hp * hn);
-  const float up = qp / hp0;
-  const float un = qn / fmaxf(fmaxf(hn, hdryl), ksat(N));
-  const float us0 = S.qx[Sx] / fmaxf(fmaxf(hs, hdryl), ksat(Sx));
-  const float use0 = S.qx[ES] / fmaxf(fmaxf(hat(ES), hdryl), ksat(ES));
-  const float une = S.qx[EN] / fmaxf(fmaxf(hat(EN), hdryl), ksat(EN));
-  const float vp = rp / hp0;
-  const float ve = re / fmaxf(fmaxf(he, hdryl), ksat(E));
-  const float vw = rw / fmaxf(fmaxf(hw, hdryl), ksat(W));
-  const float vwn = S.qy[WN] / fmaxf(fmaxf(hat(WN), hdryl), ksat(WN));
-  const float ven = S.qy[EN] / fmaxf(fmaxf(hat(EN), hdryl), ksat(EN));
+  const float cme = fsqrt(gaccl * hme), cmn = fsqrt(gaccl * hmn);
+  const float rhme = frcp(fmaxf(hme, hdryl)), rhmn = frcp(fmaxf(hmn, hdryl));
+  const float ume = qme * rhme, vme = rme * rhme;
+  const float umn = qmn * rhmn, vmn = rmn * rhmn;
+  const float hne = nueml * fsqrt(hp * he);  // (cvdef*us*h + nuem), us = 0
+  const float hnn = nueml * fsqrt(hp * hn);
+  const float rhp0 = frcp(hp0);
+  const float up = qp * rhp0;
+  const float un = fdiv(qn, fmaxf(fmaxf(hn, hdryl), ksat(N)));
+  const float us0 = fdiv(S.qx[Sx], fmaxf(fmaxf(hs, hdryl), ksat(Sx)));
+  const float use0 = fdiv(S.qx[ES], fmaxf(fmaxf(hat(ES), hdryl), ksat(ES)));
+  const float une = fdiv(S.qx[EN], fmaxf(fmaxf(hat(EN), hdryl), ksat(EN)));
+  const float vp = rp * rhp0;
+  const float ve = fdiv(re, fmaxf(fmaxf(he, hdryl), ksat(E)));
+  const float vw = fdiv(rw, fmaxf(fmaxf(hw, hdryl), ksat(W)));
+  const float vwn = fdiv(S.qy[WN], fmaxf(fmaxf(hat(WN), hdryl), ksat(WN)));
+  const float ven = fdiv(S.qy[EN], fmaxf(fmaxf(hat(EN), hdryl), ksat(EN)));
   const float txye = hne * (div_dxy_f(d, ve - vp) + div_dxy_f(d, .25f * (un + une - us0 - use0)));
   const float txyn = hnn * (div_dxy_f(d, un - up) + div_dxy_f(d, .25f * (ve + ven - vw - vwn)));
   const float fe1c = qme, fe2c = qme * ume, fe3c = qme * vme - txye;
@@ -604,7 +638,7 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
         dzea = fminf(dzea, fabsf(he - hp));
         dze = copysignf(dzea, dze);
       }
-      cc = .25f / cme;
+      cc = fdiv(.25f, cme);
     } else {
       cc = 0.0f;
     }
@@ -616,7 +650,7 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
     if (!ldp_dry && .5 * (fmax(0.0, dP) + fmax(0.0, dN)) > hdry) {
       float dzna = fminf(fabsf(dzn), fabsf(hn - hp));
       dzn = copysignf(dzna, dzn);
-      cc = .25f / cmn;
+      cc = fdiv(.25f, cmn);
     } else {
       cc = 0.0f;
     }
@@ -636,14 +670,14 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   float fn1 = fn1c + fn1r;
   const float fn2 = fn2c + fn2r;
   const float fn3 = fn3c + fn3r + .5f * gaccl * (hmn * hmn);
-  const float weir = sqrtf(gaccl) * hp * sqrtf(hp);
+  const float weir = fsqrt(gaccl) * hp * fsqrt(hp);
   if (icol == 1 || icol == d.nc) fn1 = fminf(volrat, weir);
   if (irow == 1 || irow == d.nr) fe1 = fminf(volrat, weir);
-  volrat = (float)d.arbase * hp / dtl;
+  volrat = fdiv((float)d.arbase * hp, dtl);
   if (volrat > 0.0f) {
     if (fe1 > 0.0f && fn1 > 0.0f) {
       if (fe1 * dy + fn1 * dx > volrat) {
-        const float cf = fn1 * dx / (fe1 * dy + fn1 * dx);
+        const float cf = fdiv(fn1 * dx, fe1 * dy + fn1 * dx);
         fe1 = div_dxy_f(d, (1.f - cf) * volrat);
         fn1 = div_dxy_f(d, cf * volrat);
       }
@@ -687,13 +721,13 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
         // the surface difference is positive (decided in FP64); its FP32
         // value can round to 0, where the inflow and its momentum are 0
         dze = fminf((float)dze_d, hme);
-        volrat = (float)d.dxy * he / dtl;
+        volrat = fdiv((float)d.dxy * he, dtl);
         if (dze > 0.0f) {
-          float qme = 0.296f * dze * sqrtf(gaccl * dze);
+          float qme = 0.296f * dze * fsqrt(gaccl * dze);
           hme = 0.444f * dze;
           qme = -fminf(qme, volrat);
           fe1 = qme;
-          fe2 = qme * (qme / hme) + .5f * gaccl * hme * hme;
+          fe2 = qme * fdiv(qme, hme) + .5f * gaccl * hme * hme;
         }
       }
     }
@@ -706,13 +740,13 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
         fn3 = .5f * gaccl * hmn * hmn;
       } else {
         dzn = fminf((float)dzn_d, hmn);
-        volrat = (float)d.dxy * hn / dtl;
+        volrat = fdiv((float)d.dxy * hn, dtl);
         if (dzn > 0.0f) {
-          float rmn = 0.296f * dzn * sqrtf(gaccl * dzn);
+          float rmn = 0.296f * dzn * fsqrt(gaccl * dzn);
           hmn = 0.444f * dzn;
           rmn = -fminf(rmn, volrat);
           fn1 = rmn;
-          fn3 = rmn * (rmn / hmn) + .5f * gaccl * hmn * hmn;
+          fn3 = rmn * fdiv(rmn, hmn) + .5f * gaccl * hmn * hmn;
         }
       }
     }
@@ -914,10 +948,11 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     if (d.manning_f && ld == 0 && !wall) {
       const float n = d.manning_f[gi];
       if (n != 0.0f) {
-        const float qm = sqrtf(qx * qx + qy * qy);
-        const float den = 1.0f + dtl * (float)d.gaccl * n * n * qm / (h * h * cbrtf(h));
-        qx = qx / den;
-        qy = qy / den;
+        const float qm = fsqrt(qx * qx + qy * qy);
+        const float den = 1.0f + fdiv(dtl * (float)d.gaccl * n * n * qm, h * h * fcbrt(h));
+        const float rden = frcp(den);
+        qx = qx * rden;
+        qy = qy * rden;
       }
     }
     d.eta[pcur + gi] = eta;

@@ -65,3 +65,4 @@ void fx_units_of(int dom, int nr, int nchem, int steps, std::vector<fx_unit>& ou
 int fx_ade_rows_per_strip();
 int fx_ade_threads_per_block();
 int fx_ade_max_blocks(int* out);
+int fx_ade_max_blocks_for(bool prec32, int* out);
