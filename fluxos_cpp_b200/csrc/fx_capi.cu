@@ -1,6 +1,8 @@
 // C ABI of libfluxos_gpu.so: context, device state, stepping (see
 // include/fluxos_gpu.h for the contract and the reference interfaces each
 // entry point replaces).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -118,11 +120,84 @@ void fx_fill_status(const fx_ctl& k, fx_status* st) {
   st->budget_out = k.budget_out;
 }
 
-// Copies the host descriptor of the domain to its device copy when it changed.
+// cuTensorMapEncodeTiled from the driver (the runtime links statically; the
+// entry point is looked up once).
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// One stencil field as a 3-D tensor (irow incl. the column padding, icol,
+// plane) with a box of `box_x` x (tile_rows + 2) x 1 elements.
+static int encode_field(fx_ctx* c, fx_tmap* out, const void* base, CUtensorMapDataType type, int esz,
+                        int planes, int box_x) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc) return fx_fail(c, FX_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const fx_dev& d = c->d;
+  cuuint64_t dims[3] = {(cuuint64_t)d.ld, (cuuint64_t)(d.nc + 2), (cuuint64_t)planes};
+  cuuint64_t strides[2] = {(cuuint64_t)d.ld * esz, (cuuint64_t)d.plane * esz};
+  cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)(d.tile_rows + 2), 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(reinterpret_cast<CUtensorMap*>(out), type, 3, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fx_fail(c, FX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return FX_OK;
+}
+
+// Tensor maps of the TMA-staged hydrodynamic kernel for the current fields
+// and tile shape (box widths: 40 4-byte, 36 8-byte, 64 1-byte elements).
+static int build_tmaps(fx_ctx* c) {
+  const fx_dev& d = c->d;
+  fx_tmap* m = c->tmaps.m;
+  int rc;
+  const CUtensorMapDataType F32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32, F64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  if (d.prec32) {
+    if ((rc = encode_field(c, &m[FX_TM_Z], d.eta, F32, 4, 2, 40)) ||
+        (rc = encode_field(c, &m[FX_TM_LO], d.eta_lo, F32, 4, 2, 40)) ||
+        (rc = encode_field(c, &m[FX_TM_QX], d.qx_f, F32, 4, 2, 40)) ||
+        (rc = encode_field(c, &m[FX_TM_QY], d.qy_f, F32, 4, 2, 40)) ||
+        (rc = encode_field(c, &m[FX_TM_MM], d.melt_mult_f ? (const void*)d.melt_mult_f : (const void*)d.eta, F32, 4,
+                           1, 40)))
+      return rc;
+  } else {
+    if ((rc = encode_field(c, &m[FX_TM_Z], d.z, F64, 8, 2, 36)) ||
+        (rc = encode_field(c, &m[FX_TM_LO], d.z, F64, 8, 2, 36)) ||
+        (rc = encode_field(c, &m[FX_TM_QX], d.qx, F64, 8, 2, 36)) ||
+        (rc = encode_field(c, &m[FX_TM_QY], d.qy, F64, 8, 2, 36)) ||
+        (rc = encode_field(c, &m[FX_TM_MM], d.melt_mult ? (const void*)d.melt_mult : (const void*)d.z, F64, 8, 1,
+                           36)))
+      return rc;
+  }
+  if ((rc = encode_field(c, &m[FX_TM_ZB], d.zb, F64, 8, 1, 36)) ||
+      (rc = encode_field(c, &m[FX_TM_FL], d.flags, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, d.nslot, 64)))
+    return rc;
+  if (fx_hydro_tma_blocks(d.prec32 != 0, d.tile_rows, &c->tma_blocks) != 0 || c->tma_blocks < 1)
+    return fx_fail(c, FX_ERR_CUDA, "occupancy query for the TMA-staged hydrodynamic kernel failed");
+  return FX_OK;
+}
+
+static bool tma_fits(const fx_ctx* c);
+
+// Copies the host descriptor of the domain to its device copy when it
+// changed, and rebuilds the tensor maps that point into its fields.
 int fx_sync_dev(fx_ctx* c) {
   if (!c->dev_dirty) return FX_OK;
   FX_CK(c, cudaMemcpyAsync(c->d_dev, &c->d, sizeof(fx_dev), cudaMemcpyHostToDevice, c->stream));
   FX_CK(c, cudaStreamSynchronize(c->stream));
+  if (c->use_tma && tma_fits(c)) {
+    int rc = build_tmaps(c);
+    if (rc) return rc;
+  }
   c->dev_dirty = false;
   return FX_OK;
 }
@@ -536,6 +611,13 @@ int fx_set_option(fx_ctx* c, const char* name, long long v) {
     return FX_OK;
   }
   if (!strcmp(name, "tile_rows")) return set_tile_rows(c, (int)v);
+  if (!strcmp(name, "tma")) {
+    c->use_tma = v != 0;
+    c->graph_dirty = true;
+    c->dev_dirty = true;
+    c->dev_version++;
+    return FX_OK;
+  }
   return fx_fail(c, FX_ERR_ARG, "fx_set_option: unknown option '%s'", name);
 }
 
@@ -582,11 +664,20 @@ int fx_prepare(fx_ctx* c) {
 
 // One batch of m steps: the clock and the hydrodynamics step by step, then
 // the ADE sweeps of all m steps in one launch (fx_ade.cu).
+// The staged kernel's boxes (64 rows of flags, tile_rows + 2 columns) must
+// fit in the field; smaller grids use the per-tile kernel.
+static bool tma_fits(const fx_ctx* c) { return c->d.ld >= 64 && c->d.nc + 2 >= c->d.tile_rows + 2; }
+
+static void launch_hydro(fx_ctx* c) {
+  if (c->use_tma && tma_fits(c)) fx_launch_hydro_tma(c->d, c->tmaps, c->tma_blocks, c->stream);
+  else fx_launch_hydro_one(c->d, c->stream);
+}
+
 static void launch_batch(fx_ctx* c, int m) {
   fx_launch_batch_begin(c->d_dev, 1, c->stream);
   for (int i = 0; i < m; ++i) {
     fx_launch_finalize(c->d_dev, 1, c->stream);
-    fx_launch_hydro_one(c->d, c->stream);
+    launch_hydro(c);
   }
   fx_launch_ade_one(c->d, c->nunits, c->ade_blocks, c->stream);
 }
@@ -740,7 +831,7 @@ int fx_time_steps(fx_ctx* c, int n, double* ms_total, double* ms_hydro, double* 
     for (int i = 0; i < m && !erc; ++i) {
       fx_launch_finalize(c->d_dev, 1, c->stream);
       if ((erc = record(&a))) break;
-      fx_launch_hydro_one(c->d, c->stream);
+      launch_hydro(c);
       if ((erc = record(&b))) break;
       hyd.push_back({a, b});
     }

@@ -199,3 +199,22 @@ __host__ __device__ inline double fx_dd_val(float hi, float lo) { return (double
 __host__ __device__ inline long long fx_pp(const fx_dev& d, long long step) {
   return (step & 1) * d.plane;
 }
+
+// Tensor maps of the TMA-staged hydrodynamic kernel (fx_hydro.cu
+// k_hydro_tma): the stencil fields as 3-D tensors (irow with the column
+// padding, icol, plane). Built on the host (fx_capi.cu fx_build_tmaps).
+#define FX_TM_Z 0   // z (FP64) or eta (FP32), two planes
+#define FX_TM_LO 1  // eta_lo (FP32), two planes
+#define FX_TM_ZB 2  // zb, one plane
+#define FX_TM_QX 3  // qx, two planes
+#define FX_TM_QY 4  // qy, two planes
+#define FX_TM_MM 5  // melt multiplier, one plane (when set)
+#define FX_TM_FL 6  // flags, nslot planes
+#define FX_TM_COUNT 7
+struct alignas(64) fx_tmap {
+  unsigned long long opaque[16];  // a CUtensorMap
+};
+struct fx_tmaps {
+  fx_tmap m[FX_TM_COUNT];
+};
+

@@ -433,6 +433,41 @@ __device__ void reduce_courant(const fx_dev& d, SM& S, double dtc, double hm) {
   }
 }
 
+// Shared-memory staging of a tile's stencil by TMA (k_hydro_tma). Each field
+// of the stencil (rows irow0-2..irow0+TX, columns icol0-2..icol0+TY) arrives
+// as one box of W elements x (BY+2) columns. A TMA box must start on a
+// 16-byte boundary along irow, so the box starts at the stencil's first row
+// rounded down to 4 (4-byte elements), 2 (8-byte) or 16 (1-byte) elements,
+// and the stencil sits `xo` elements into it. Rows and columns outside the
+// field read 0 (TMA out-of-bounds fill; the field padding is 0 as well), as
+// the per-thread loads of the unstaged path do.
+constexpr int STG_W4 = 40, STG_W8 = 36, STG_W1 = 64;  // box widths: 34 + largest offset, 16-byte multiples
+__host__ __device__ constexpr int stg_round(int b) { return (b + 127) / 128 * 128; }
+template <bool P32, int BY>
+struct StageLayout {
+  static constexpr int SY = BY + 2;
+  static constexpr int B4 = stg_round(STG_W4 * SY * 4), B8 = stg_round(STG_W8 * SY * 8), B1 = stg_round(STG_W1 * SY);
+  // FP64 stage: z, zb, qx, qy, melt multiplier (8-byte boxes), flags (1-byte)
+  // FP32 stage: eta, eta_lo, qx, qy, melt multiplier (4-byte boxes), zb (8-byte), flags
+  static constexpr int O_Z = 0;                                   // z | eta
+  static constexpr int O_LO = P32 ? B4 : 0;                       // - | eta_lo
+  static constexpr int O_ZB = P32 ? 2 * B4 : B8;                  // zb
+  static constexpr int O_QX = P32 ? 2 * B4 + B8 : 2 * B8;         // qx
+  static constexpr int O_QY = P32 ? 3 * B4 + B8 : 3 * B8;         // qy
+  static constexpr int O_MM = P32 ? 4 * B4 + B8 : 4 * B8;         // melt multiplier
+  static constexpr int O_FL = P32 ? 5 * B4 + B8 : 5 * B8;         // flags
+  static constexpr int BYTES = O_FL + B1;
+};
+
+// x offsets of the stencil in the staged boxes of tile column bx.
+struct StageOff {
+  int o4, o8, o1;
+};
+__device__ __forceinline__ StageOff stage_off(int bx) {
+  const int x = TX * bx;  // element index of stencil row 0: irow0 - 2 + FX_ROFF
+  return StageOff{x & 3, x & 1, x & 15};
+}
+
 // The fields of the control block a step kernel reads.
 struct StepCtl {
   double dtfl, meteoi, meteo_rate, mconc;
@@ -764,7 +799,9 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
 
 template <int BY>
 __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
-                                             HydroSmem32<BY>& S) {
+                                             HydroSmem32<BY>& S, const unsigned char* stg = nullptr) {
+  using L = StageLayout<true, BY>;
+  const StageOff so = stage_off(tile.bx);
   constexpr int TY = Tile<BY>::TY, NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX;
   constexpr int NTHREADS = Tile<BY>::NTHREADS;
   const int lx = threadIdx.x, ly = threadIdx.y;
@@ -821,6 +858,43 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     S.ndry = 0;
     S.nstale = 0;
   }
+  if (stg) {
+    // staged by TMA: the same values, read from shared memory
+    const float* g_eta = reinterpret_cast<const float*>(stg + L::O_Z);
+    const float* g_lo = reinterpret_cast<const float*>(stg + L::O_LO);
+    const double* g_zb = reinterpret_cast<const double*>(stg + L::O_ZB);
+    const float* g_qx = reinterpret_cast<const float*>(stg + L::O_QX);
+    const float* g_qy = reinterpret_cast<const float*>(stg + L::O_QY);
+    const float* g_mm = reinterpret_cast<const float*>(stg + L::O_MM);
+    const uint8_t* g_fl = stg + L::O_FL;
+    for (int k = tid; k < NSTEN; k += NTHREADS) {
+      const int sr = k % SX, scc = k / SX;
+      const int r = irow0 - 2 + sr, q = icol0 - 2 + scc;
+      const int i4 = scc * STG_W4 + sr + so.o4;
+      float eta = g_eta[i4], lo = g_lo[i4], qx = g_qx[i4], qy = g_qy[i4];
+      const double zb = g_zb[scc * STG_W8 + sr + so.o8];
+      unsigned char cl = 0;
+      if (r >= 1 && r <= d.nr && q >= 1 && q <= d.nc) {
+        cl = C_INT;
+        const uint8_t fl = g_fl[scc * STG_W1 + sr + so.o1];
+        if (fl & FX_F_WALL) cl |= C_WALL;
+        if (melt_on && !(fl & FX_F_NODATA))
+          fx_dd_add(eta, lo, (float)(d.melt_mult_f ? (double)c.meteo_rate * (double)g_mm[i4] / (1000. * 3600. * 24.) * c.dtfl
+                                                   : c.meteoi));
+        if (fx_dd_val(eta, lo) <= d.hdry) {
+          qx = 0.f;
+          qy = 0.f;
+          cl |= C_DRY;
+        }
+      }
+      S.eta[k] = eta;
+      S.eta_lo[k] = lo;
+      S.zb[k] = zb;
+      S.qx[k] = qx;
+      S.qy[k] = qy;
+      S.cls[k] = cl;
+    }
+  } else
   for (int k = tid; k < NSTEN; k += NTHREADS) {
     const int sr = k % SX, scc = k / SX;
     const int r = irow0 - 2 + sr, q = icol0 - 2 + scc;
@@ -905,14 +979,18 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     const int fP = (ly + 1) * FXN + (lx + 1), fW = (ly + 1) * FXN + lx, fS = ly * FXN + (lx + 1);
     const unsigned char cl = S.cls[sP];
     const bool wall = cl & C_WALL;
-    const uint8_t fl = d.flags[sprev + gi];
+    const int i4 = (ly + 2) * STG_W4 + lx + 2 + so.o4;
+    const uint8_t fl = stg ? stg[L::O_FL + (ly + 2) * STG_W1 + lx + 2 + so.o1] : d.flags[sprev + gi];
     const float eta1 = S.eta[sP];
-    const float etapre = d.eta[pprev + gi];
+    const float etapre = stg ? reinterpret_cast<const float*>(stg + L::O_Z)[i4] : d.eta[pprev + gi];
     float h0v = fmaxf(0.0f, etapre);
     if (melt_on && !(fl & FX_F_NODATA)) {
       h0v = fmaxf(eta1, 0.0f);
       if (d.ade) d.hpm_f[scur + gi] = fmaxf(etapre, 0.0f);
-      bmelt = melt_depth(d, c, gi) * d.arbase;
+      bmelt = (stg && d.melt_mult_f)
+                  ? (double)c.meteo_rate * (double)reinterpret_cast<const float*>(stg + L::O_MM)[i4] /
+                        (1000. * 3600. * 24.) * c.dtfl * d.arbase
+                  : melt_depth(d, c, gi) * d.arbase;
     }
     if (!(cl & C_DRY)) d.twet_f[gi] += (float)(c.dtfl / 3600);
     float dh = 0.f, dqx = 0.f, dqy = 0.f, qxfP = 0.f, qyfP = 0.f;
@@ -987,7 +1065,9 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
 // The FP64 step of one tile (the reference's arithmetic, bit for bit).
 template <int BY>
 __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
-                                             HydroSmem<BY>& S) {
+                                             HydroSmem<BY>& S, const unsigned char* stg = nullptr) {
+  using L = StageLayout<false, BY>;
+  const StageOff so = stage_off(tile.bx);
   constexpr int TY = Tile<BY>::TY, NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX;
   constexpr int NTHREADS = Tile<BY>::NTHREADS;
   const int lx = threadIdx.x, ly = threadIdx.y;
@@ -1049,6 +1129,40 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     S.ndry = 0;
     S.nstale = 0;
   }
+  if (stg) {
+    // staged by TMA: the same values, read from shared memory
+    const double* g_z = reinterpret_cast<const double*>(stg + L::O_Z);
+    const double* g_zb = reinterpret_cast<const double*>(stg + L::O_ZB);
+    const double* g_qx = reinterpret_cast<const double*>(stg + L::O_QX);
+    const double* g_qy = reinterpret_cast<const double*>(stg + L::O_QY);
+    const double* g_mm = reinterpret_cast<const double*>(stg + L::O_MM);
+    const uint8_t* g_fl = stg + L::O_FL;
+    for (int k = tid; k < NSTEN; k += NTHREADS) {
+      const int sr = k % SX, sc = k / SX;
+      const int r = irow0 - 2 + sr, q = icol0 - 2 + sc;
+      const int i8 = sc * STG_W8 + sr + so.o8;
+      double z = g_z[i8], qx = g_qx[i8], qy = g_qy[i8];
+      const double zb = g_zb[i8];
+      unsigned char cl = 0;
+      if (r >= 1 && r <= d.nr && q >= 1 && q <= d.nc) {
+        cl = C_INT;
+        if (g_fl[sc * STG_W1 + sr + so.o1] & FX_F_WALL) cl |= C_WALL;
+        if (melt_on && zb != d.nodata)
+          z = z + (d.melt_mult ? (double)c.meteo_rate * g_mm[i8] / (1000. * 3600. * 24.) * c.dtfl : c.meteoi);
+        const double h1 = fmax(0.0, z - zb);
+        if (h1 <= d.hdry) {
+          qx = 0.0;
+          qy = 0.0;
+          cl |= C_DRY;
+        }
+      }
+      S.z[k] = z;
+      S.zb[k] = zb;
+      S.qx[k] = qx;
+      S.qy[k] = qy;
+      S.cls[k] = cl;
+    }
+  } else
   for (int k = tid; k < NSTEN; k += NTHREADS) {
     const int sr = k % SX, sc = k / SX;
     const int r = irow0 - 2 + sr, q = icol0 - 2 + sc;
@@ -1141,10 +1255,11 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     const int fP = (ly + 1) * FXN + (lx + 1), fW = (ly + 1) * FXN + lx, fS = ly * FXN + (lx + 1);
     const unsigned char cl = S.cls[sP];
     const bool wall = cl & C_WALL;
-    const uint8_t fl = d.flags[sprev + gi];
+    const int i8 = (ly + 2) * STG_W8 + lx + 2 + so.o8;
+    const uint8_t fl = stg ? stg[L::O_FL + (ly + 2) * STG_W1 + lx + 2 + so.o1] : d.flags[sprev + gi];
     const double zb = S.zb[sP];
     const double z1 = S.z[sP];
-    const double zpre = d.z[pprev + gi];
+    const double zpre = stg ? reinterpret_cast<const double*>(stg + L::O_Z)[i8] : d.z[pprev + gi];
 
     // add_meteo's h0 (common.cpp:223): the depth after the melt, or the
     // Courant scan's copy of h (main.cpp:305) for cells it skips. Its solute
@@ -1153,7 +1268,10 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     if (melt_on && zb != d.nodata) {
       h0v = fmax(z1 - zb, 0.0);
       if (d.ade) d.hpm[scur + gi] = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
-      bmelt = melt_depth(d, c, gi) * d.arbase;
+      bmelt = (stg && d.melt_mult)
+                  ? (double)c.meteo_rate * reinterpret_cast<const double*>(stg + L::O_MM)[i8] /
+                        (1000. * 3600. * 24.) * c.dtfl * d.arbase
+                  : melt_depth(d, c, gi) * d.arbase;
     }
     // Loop 1 wet time (:69-70)
     if (!(cl & C_DRY)) d.twet[gi] += dtl / 3600;
@@ -1299,6 +1417,150 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>()) k_hydro_batch(
   hydro_block<P32, BY>(sd, tile, S, sc);
 }
 static_assert(sizeof(fx_dev) % 8 == 0, "descriptor copied as 8-byte words");
+
+// ---- TMA-staged persistent form -------------------------------------------
+// One block per SM slot loops over the domain's tiles. Thread 0 loads the
+// stencil of the block's next tile into the other of two shared-memory
+// stages with TMA (cp.async.bulk.tensor, completion counted on an mbarrier)
+// while the block computes the current one, so the halo reads of a tile
+// overlap the arithmetic of the previous tile.
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, int y, int z,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Issue the loads of tile t's stencil into stage `stg` (thread 0).
+template <bool P32, int BY>
+__device__ __forceinline__ void stage_issue(const fx_dev& d, const fx_tmaps& tm, int t, int ntx, long long step_prev,
+                                            unsigned char* stg, unsigned long long* bar) {
+  using L = StageLayout<P32, BY>;
+  const int bx = t % ntx, by = t / ntx;
+  const int x = TX * bx, y = (BY - 1) * by - 1;  // stencil origin (irow0 - 2 + FX_ROFF, icol0 - 2)
+  const int x4 = x & ~3, x8 = x & ~1, x1 = x & ~15;
+  const int pp = (int)(step_prev & 1), sl = (int)(step_prev % d.nslot);
+  const bool mm = P32 ? d.melt_mult_f != nullptr : d.melt_mult != nullptr;
+  const unsigned bytes = (unsigned)((P32 ? 4 * STG_W4 * L::SY * 4 + STG_W8 * L::SY * 8
+                                         : 4 * STG_W8 * L::SY * 8) +
+                                    (mm ? (P32 ? STG_W4 * L::SY * 4 : STG_W8 * L::SY * 8) : 0) + STG_W1 * L::SY);
+  mbar_expect_tx(bar, bytes);
+  if (P32) {
+    tma_load_3d(stg + L::O_Z, &tm.m[FX_TM_Z], x4, y, pp, bar);
+    tma_load_3d(stg + L::O_LO, &tm.m[FX_TM_LO], x4, y, pp, bar);
+    tma_load_3d(stg + L::O_ZB, &tm.m[FX_TM_ZB], x8, y, 0, bar);
+    tma_load_3d(stg + L::O_QX, &tm.m[FX_TM_QX], x4, y, pp, bar);
+    tma_load_3d(stg + L::O_QY, &tm.m[FX_TM_QY], x4, y, pp, bar);
+    if (mm) tma_load_3d(stg + L::O_MM, &tm.m[FX_TM_MM], x4, y, 0, bar);
+  } else {
+    tma_load_3d(stg + L::O_Z, &tm.m[FX_TM_Z], x8, y, pp, bar);
+    tma_load_3d(stg + L::O_ZB, &tm.m[FX_TM_ZB], x8, y, 0, bar);
+    tma_load_3d(stg + L::O_QX, &tm.m[FX_TM_QX], x8, y, pp, bar);
+    tma_load_3d(stg + L::O_QY, &tm.m[FX_TM_QY], x8, y, pp, bar);
+    if (mm) tma_load_3d(stg + L::O_MM, &tm.m[FX_TM_MM], x8, y, 0, bar);
+  }
+  tma_load_3d(stg + L::O_FL, &tm.m[FX_TM_FL], x1, y, sl, bar);
+}
+
+constexpr long long STAGE_SPIN_LIMIT = 1LL << 22;  // polls of a stage's mbarrier before giving up
+
+template <bool P32, int BY>
+__global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
+    k_hydro_tma(const __grid_constant__ fx_dev d, const __grid_constant__ fx_tmaps tm, int ntx, int nty) {
+  using L = StageLayout<P32, BY>;
+  __shared__ HydroSmem<BY> S;
+  __shared__ StepCtl sc;
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ int abort_flag;
+  extern __shared__ __align__(128) unsigned char dyn[];
+  unsigned char* stage0 = dyn + ((128 - (smem_u32(dyn) & 127)) & 127);
+  const int tid = threadIdx.y * BX + threadIdx.x;
+  const int ntiles = ntx * nty;
+  if (tid == 0) {
+    const fx_ctl& g = *d.ctl;
+    sc.dtfl = g.dtfl;
+    sc.meteoi = g.meteoi;
+    sc.meteo_rate = g.meteo_rate;
+    sc.mconc = g.mconc;
+    sc.steps = g.steps;
+    sc.live = g.live;
+    sc.active = g.active;
+    abort_flag = 0;
+  }
+  __syncthreads();
+  const StepCtl c = sc;
+  if (!c.live) return;
+  if (!c.active) {  // no solver this step: cell-local work only, nothing to stage
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const fx_tile tile{0, t % ntx, t / ntx, 0};
+      if constexpr (P32) hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S));
+      else hydro_tile64<BY>(d, c, tile, S);
+      __syncthreads();
+    }
+    return;
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (blockIdx.x < ntiles) stage_issue<P32, BY>(d, tm, blockIdx.x, ntx, c.steps - 1, stage0, &bar[0]);
+  }
+  __syncthreads();
+  unsigned parity = 0u;  // bit q: phase of stage q's barrier
+  int st = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    if (tid == 0 && tn < ntiles)
+      stage_issue<P32, BY>(d, tm, tn, ntx, c.steps - 1, stage0 + (st ^ 1) * L::BYTES, &bar[st ^ 1]);
+    // wait for this tile's stencil, bounded
+    long long it = 0;
+    while (!mbar_try_wait(&bar[st], (parity >> st) & 1u)) {
+      if (++it > STAGE_SPIN_LIMIT) {
+        abort_flag = 1;
+        break;
+      }
+    }
+    parity ^= 1u << st;
+    __syncthreads();
+    if (abort_flag) {
+      if (tid == 0) {
+        atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
+        // let the copy of the next tile, if one was issued, land before the block exits
+        long long w = 0;
+        if (tn < ntiles)
+          while (!mbar_try_wait(&bar[st ^ 1], (parity >> (st ^ 1)) & 1u) && ++w < STAGE_SPIN_LIMIT) {
+          }
+      }
+      return;
+    }
+    const fx_tile tile{0, t % ntx, t / ntx, 0};
+    if constexpr (P32)
+      hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S), stage0 + st * L::BYTES);
+    else hydro_tile64<BY>(d, c, tile, S, stage0 + st * L::BYTES);
+    __syncthreads();  // the stage is free for the load issued two tiles later
+    st ^= 1;
+  }
+}
 
 // Courant scan of the state as uploaded (the scan at the top of the first
 // step). Also used after a host edit of the state.
@@ -1495,6 +1757,45 @@ void fx_launch_hydro_one(const fx_dev& d, cudaStream_t s) {
   else if (d.tile_rows == 16) launch_hydro_one<16>(d, s);
   else launch_hydro_one<8>(d, s);
 }
+namespace {
+template <int BY>
+void launch_hydro_tma(const fx_dev& d, const fx_tmaps& tm, int nblocks, cudaStream_t s) {
+  const int ntx = (d.nr + fx::TX - 1) / fx::TX, nty = (d.nc + fx::Tile<BY>::TY - 1) / fx::Tile<BY>::TY;
+  const size_t dyn = (size_t)2 * (d.prec32 ? fx::StageLayout<true, BY>::BYTES : fx::StageLayout<false, BY>::BYTES) + 128;
+  if (d.prec32) fx::k_hydro_tma<true, BY><<<nblocks, dim3(fx::BX, BY), dyn, s>>>(d, tm, ntx, nty);
+  else fx::k_hydro_tma<false, BY><<<nblocks, dim3(fx::BX, BY), dyn, s>>>(d, tm, ntx, nty);
+}
+template <bool P32, int BY>
+int tma_blocks(int* out) {
+  const size_t dyn = (size_t)2 * fx::StageLayout<P32, BY>::BYTES + 128;
+  if (cudaFuncSetAttribute(fx::k_hydro_tma<P32, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) !=
+      cudaSuccess)
+    return -1;
+  int dev = 0, nsm = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fx::k_hydro_tma<P32, BY>, fx::BX * BY, dyn) !=
+      cudaSuccess)
+    return -1;
+  *out = per * nsm;
+  return 0;
+}
+}  // namespace
+
+void fx_launch_hydro_tma(const fx_dev& d, const fx_tmaps& tm, int nblocks, cudaStream_t s) {
+  if (d.tile_rows == 4) launch_hydro_tma<4>(d, tm, nblocks, s);
+  else if (d.tile_rows == 16) launch_hydro_tma<16>(d, tm, nblocks, s);
+  else launch_hydro_tma<8>(d, tm, nblocks, s);
+}
+
+// Resident blocks of the TMA-staged hydrodynamic kernel (after raising its
+// dynamic shared memory limit); the persistent grid is at most this.
+int fx_hydro_tma_blocks(bool prec32, int tile_rows, int* out) {
+  if (tile_rows == 4) return prec32 ? tma_blocks<true, 4>(out) : tma_blocks<false, 4>(out);
+  if (tile_rows == 16) return prec32 ? tma_blocks<true, 16>(out) : tma_blocks<false, 16>(out);
+  return prec32 ? tma_blocks<true, 8>(out) : tma_blocks<false, 8>(out);
+}
+
 void fx_launch_courant_scan(const fx_dev* devs, const fx_tile* tiles, int ntiles, int tile_rows, cudaStream_t s) {
   if (tile_rows == 4) fx::k_courant_scan<4><<<ntiles, dim3(fx::BX, 4), 0, s>>>(devs, tiles);
   else if (tile_rows == 16) fx::k_courant_scan<16><<<ntiles, dim3(fx::BX, 16), 0, s>>>(devs, tiles);

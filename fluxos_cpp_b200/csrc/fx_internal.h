@@ -37,6 +37,11 @@ struct fx_ctx {
   // the bed then on the device.
   std::vector<double> z_pending;
   double* d_mass = nullptr;    // fx_mass result: water, then one mass per solute
+  // TMA-staged hydrodynamic kernel (one domain): tensor maps of the stencil
+  // fields, rebuilt with the descriptor; its persistent grid size
+  fx_tmaps tmaps{};
+  bool use_tma = true;
+  int tma_blocks = 0;
   // file surface (filled by fx_open_modset)
   double h_min_print = 0.0;
   std::string output_folder;
@@ -54,6 +59,8 @@ void fx_launch_mark_static(const fx_dev* devs, int dom, cudaStream_t s);
 void fx_launch_hydro(const fx_dev* devs, const fx_tile* tiles, int ntiles, bool prec32, int tile_rows,
                      cudaStream_t s);
 void fx_launch_hydro_one(const fx_dev& d, cudaStream_t s);
+void fx_launch_hydro_tma(const fx_dev& d, const fx_tmaps& tm, int nblocks, cudaStream_t s);
+int fx_hydro_tma_blocks(bool prec32, int tile_rows, int* out);
 void fx_launch_courant_scan(const fx_dev* devs, const fx_tile* tiles, int ntiles, int tile_rows, cudaStream_t s);
 void fx_launch_ade(const fx_dev* devs, const fx_unit* units, int nunits, int nblocks, bool prec32, cudaStream_t s);
 void fx_launch_ade_one(const fx_dev& d, int nunits, int nblocks, cudaStream_t s);

@@ -124,7 +124,10 @@ int fx_set_melt_field(fx_ctx* ctx, const double* mult_grid);
  * device every step; 0, the default, skips those stores for cells that end a
  * step wet, whose values are never read back by a later step);
  * "tile_rows" (4, 8 or 16: hydrodynamic tiles of 31 x (tile_rows - 1) cells,
- * 32 x tile_rows threads; default 8). Results do not depend on tile_rows. */
+ * 32 x tile_rows threads; default 8); "tma" (1, the default: a persistent
+ * hydrodynamic kernel whose blocks stage each tile's stencil into shared
+ * memory by TMA while computing the previous tile; 0: one block per tile
+ * loading its stencil itself). Results depend on neither. */
 int fx_set_option(fx_ctx* ctx, const char* name, long long value);
 int fx_prepare(fx_ctx* ctx);
 

@@ -98,17 +98,18 @@ def _fractal_wet(n, seed):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_tile_shapes_and_autotuner_keep_results(precision):
+def test_tile_shapes_staging_and_autotuner_keep_results(precision):
     sc = _fractal_wet(150, 11)
     ref = S.make_domain(sc, precision=precision, steps_in_flight=4)
     ref.step(40)
     want = {k: ref.download(k) for k in ("z", "h", "qx", "qy", "conc")}
-    for r in (4, 16):
+    for r, tma in ((4, 1), (16, 1), (8, 0), (16, 0)):
         d = S.make_domain(sc, precision=precision, steps_in_flight=4)
         d.set_option("tile_rows", r)
+        d.set_option("tma", tma)  # TMA-staged persistent kernel or one block per tile
         d.step(40)
         for k, v in want.items():
-            assert np.array_equal(d.download(k), v), (r, k)
+            assert np.array_equal(d.download(k), v), (r, tma, k)
         d.close()
     d = S.make_domain(sc, precision=precision, steps_in_flight=4)
     assert d.autotune(8) in (4, 8, 16)
