@@ -303,13 +303,13 @@ def run_mix(args, peak: float) -> dict:
     steps = args.mix_steps
 
     def batch_rate(precision):
-        doms = [S.make_domain(sc, precision=precision, steps_in_flight=args.in_flight) for sc in scs]
+        doms = [S.make_domain(sc, precision=precision, steps_in_flight=args.mix_in_flight) for sc in scs]
         b = fx.Batch()
         for d in doms:
             b.add(d)
-        tuned = b.autotune(4) if precision == "fp32" else (8, args.in_flight)
+        tuned = b.autotune(4) if precision == "fp32" else (8, args.mix_in_flight)
         if precision == "fp64":
-            b.set_option("steps_in_flight", args.in_flight)
+            b.set_option("steps_in_flight", args.mix_in_flight)
         b.step(args.warmup)
         s0 = [d.status()["steps"] for d in doms]
         stream = torch.cuda.ExternalStream(b.stream())
@@ -332,7 +332,7 @@ def run_mix(args, peak: float) -> dict:
     # plain FP64 path: each scenario alone, one after another
     tot_ms, tot_cells = 0.0, 0
     for sc, c in zip(scs, cells):
-        d = S.make_domain(sc, precision="fp64", steps_in_flight=args.in_flight)
+        d = S.make_domain(sc, precision="fp64", steps_in_flight=args.mix_in_flight)
         d.step(args.warmup)
         s0 = d.status()["steps"]
         ms, _, _ = d.time_steps(steps)
@@ -480,7 +480,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=63)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--size", type=int, default=4096)
@@ -488,7 +488,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-crop", type=int, default=2048)
     ap.add_argument("--cpu-steps", type=int, default=12)
-    ap.add_argument("--in-flight", type=int, default=31, help="steps per ADE launch (1..31)")
+    ap.add_argument("--in-flight", type=int, default=63, help="steps per ADE launch (1..63)")
+    ap.add_argument("--mix-in-flight", type=int, default=31,
+                    help="steps in flight of the ensemble members (memory: slot planes per step)")
     ap.add_argument("--precision", default="both", choices=("both", "fp64", "fp32"),
                     help="both: FP32 headline with FP64 beside it and the FP32 error")
     ap.add_argument("--no-mix", action="store_true")

@@ -47,8 +47,10 @@ namespace fxade {
 constexpr int ROWS = 30;      // rows per strip (lanes 0..29 compute)
 constexpr int WARPS = 4;      // warps per block
 constexpr int CHUNK = 4;      // steps between progress checks and publications
-constexpr int RING = 8;       // per-lane prefetch slots (a power of two)
-constexpr int DIST = 4;       // prefetch distance in columns (< RING)
+constexpr int RING = 4;       // per-lane prefetch slots (a power of two); a deeper ring takes shared
+                              // memory from L1, which the lanes' skewed reads depend on (measured:
+                              // 8 slots made the FP64 sweep 2.5x slower)
+constexpr int DIST = 2;       // prefetch distance in columns (< RING)
 constexpr long long SPIN_LIMIT = 1LL << 20;  // polls (well under a second) before giving up
 
 // Per-lane ring of prefetched cells, filled by cp.async (asynchronous
@@ -457,10 +459,13 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
     auto need_p1 = [&](int col) { return min(col + 2, TW); };
     if (!wait_deps(d, dep, min(CHUNK - 1 + ROWS, TW), need_p0(DIST + 3), need_p1(DIST + 3))) bail = true;
 
-    // prime the ring: columns iy0 .. iy0 + DIST + 2 of this lane's row
+    // prime: the first three columns of this lane's row become records, then
+    // columns iy0 + 3 .. iy0 + DIST + 2 go in flight (the ring holds only the
+    // DIST + 1 columns in flight, so RING >= DIST + 1)
+    static_assert(RING >= DIST + 1, "ring too shallow for the prefetch distance");
     const int iy0 = 1 - lane;
     if (!bail) {
-      for (int j = 0; j < DIST + 3; ++j) {
+      for (int j = 0; j < 3; ++j) {
         prefetch<T>(d, S, A, R, lane, ix, iy0 + j);
         cp_commit();
       }
@@ -469,6 +474,12 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
     Rec<T> cur = make_rec<T>(d, S, R, lane, ix, iy0);
     Rec<T> n1 = make_rec<T>(d, S, R, lane, ix, iy0 + 1);
     Rec<T> n2 = make_rec<T>(d, S, R, lane, ix, iy0 + 2);
+    if (!bail) {
+      for (int j = 3; j < DIST + 3; ++j) {
+        prefetch<T>(d, S, A, R, lane, ix, iy0 + j);
+        cp_commit();
+      }
+    }
     // carries: outputs of this lane's previous cell (its south cell for the
     // next step, its west cell for lane + 1)
     T o_c = T(0), o_pfe = T(0), o_b = T(0), o_qfn = T(0);

@@ -248,7 +248,7 @@ int fx_batch_set_option(fx_batch* b, const char* name, long long v) {
     if (!fx_tile_rows_ok((int)v)) return fx_fail(nullptr, FX_ERR_ARG, "tile_rows must be 4, 8 or 16");
     b->tile_rows = (int)v;
   } else if (!strcmp(name, "steps_in_flight")) {
-    if (v < 1 || v > FX_MAX_SLOTS - 1) return fx_fail(nullptr, FX_ERR_ARG, "steps_in_flight must be 1..31");
+    if (v < 1 || v > FX_MAX_SLOTS - 1) return fx_fail(nullptr, FX_ERR_ARG, "steps_in_flight must be 1..63");
     b->k_limit = (int)v;
   } else {
     return fx_fail(nullptr, FX_ERR_ARG, "fx_batch_set_option: unknown option '%s'", name);

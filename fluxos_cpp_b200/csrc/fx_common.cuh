@@ -14,7 +14,7 @@
 #define FX_ROFF 1
 #define FX_MAX_CHEM 8
 #define FX_METEO_ROWS 2000
-#define FX_MAX_SLOTS 32
+#define FX_MAX_SLOTS 64
 
 // Per-cell flag byte.
 #define FX_F_LDRY 0x01       // ldry (1 = dry) at the end of the last step

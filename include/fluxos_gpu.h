@@ -63,7 +63,7 @@ typedef struct fx_params {
   int ade;           /* EXTERNAL_MODULES.ADE_TRANSPORT.STATUS */
   int volrat_mode;   /* domain-edge weir: 0 = weir formula (default), 1 = closed */
   double d_coef[FX_MAX_CHEM]; /* dispersion coefficient per solute */
-  int steps_in_flight; /* steps whose ADE sweeps run in one launch, 1..31 (0 = 8) */
+  int steps_in_flight; /* steps whose ADE sweeps run in one launch, 1..63 (0 = 8) */
   int precision;       /* 0 = FP64, the reference's arithmetic (default);
                           1 = FP32 state: the depth above the bed eta = z - zb and
                           the bed's differences to the east and north neighbours
@@ -178,7 +178,7 @@ int fx_batch_step(fx_batch* b, int nsteps, fx_status* st);
 void* fx_batch_stream(fx_batch* b);
 /* Options of the batch's launches: "tile_rows" (4, 8, 16, as for
  * fx_set_option) and "steps_in_flight" (upper bound on the steps per graph,
- * 1..31; the members' own steps_in_flight bound it too). */
+ * 1..63; the members' own steps_in_flight bound it too). */
 int fx_batch_set_option(fx_batch* b, const char* name, long long value);
 /* Autotuner of the batch: tries each tile shape, then each steps-in-flight
  * bound, for trial_steps real steps of all members, keeps the fastest
