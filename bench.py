@@ -62,8 +62,8 @@ ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
 # case of this workload, one launch, divided by the cells and the steps the
 # launch covers); traffic scales with the cells, so `traffic` in the line is
 # this times the cells of the run.
-DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 125.24, "k_ade_sweep": 47.01},
-                       "fp32": {"k_hydro": 72.81, "k_ade_sweep": 23.86}}
+DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 125.95, "k_ade_sweep": 61.35},
+                       "fp32": {"k_hydro": 72.40, "k_ade_sweep": 25.33}}
 
 
 def _rank():
