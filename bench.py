@@ -250,8 +250,10 @@ def cpu_reference_run(sc, h, conc, warmup: int, steps: int, crop: int):
 
 
 def measure_domain(d, steps: int, warmup: int, cells: int, precision: str, peak: float, gpu: str):
-    """Warm-up, then `steps` timed steps (CUDA events on the domain's stream
-    around every launch, fx_time_steps); roofline of the dominant kernel."""
+    """Autotune the tile shape (real steps, part of the warm-up), warm-up,
+    then `steps` timed steps (CUDA events on the domain's stream around every
+    launch, fx_time_steps); roofline of the dominant kernel."""
+    tile_rows = d.autotune(8)
     d.step(warmup)
     sampler = ClockSampler(gpu)
     sampler.start()
@@ -273,7 +275,7 @@ def measure_domain(d, steps: int, warmup: int, cells: int, precision: str, peak:
             "ms_per_step": {"k_hydro": round(ms_h, 4), "k_ade_sweep": round(ms_a, 4)},
             "step_alg_GBps": round(cells * alg["step"] / (ms_total / steps / 1e3) / 1e9, 1)}
     return {"ms_total": ms_total, "value": cells * steps / (ms_total / 1e3), "roofline": roof,
-            "clocks": clocks}
+            "clocks": clocks, "tile_rows": tile_rows}
 
 
 def accuracy_of(d32, d64, w32: float, w64: float, hdry: float) -> dict:
@@ -303,7 +305,10 @@ def run_mix(args, peak: float) -> dict:
     steps = args.mix_steps
 
     def batch_rate(precision):
-        doms = [S.make_domain(sc, precision=precision, steps_in_flight=args.mix_in_flight) for sc in scs]
+        # FP32 members hold 63 steps in flight (82 GB for the 64 scenarios); FP64 ones
+        # args.mix_in_flight (memory: FP64 slot planes are twice as large)
+        k_members = 63 if precision == "fp32" else args.mix_in_flight
+        doms = [S.make_domain(sc, precision=precision, steps_in_flight=k_members) for sc in scs]
         b = fx.Batch()
         for d in doms:
             b.add(d)
@@ -439,9 +444,11 @@ def run_gpu(args):
                            "l2": "inputs larger than L2 (4-8 GB of state per replica)",
                            "parallelism": f"replicas x{world}"},
                 "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res[head]["clocks"],
-                "cpu_baseline": cpu, "accuracy": acc}
+                "cpu_baseline": cpu, "accuracy": acc,
+                "autotuned": {"tile_rows": res[head]["tile_rows"]}}
         if "fp64" in res and head != "fp64":
             line["fp64"] = {"value": res["fp64"]["value"], "ms_per_step": res["fp64"]["ms_total"] / args.steps,
+                            "autotuned": {"tile_rows": res["fp64"]["tile_rows"]},
                             "roofline": res["fp64"]["roofline"], "clocks": res["fp64"]["clocks"]}
             line["fp32_over_fp64"] = round(res[head]["value"] / res["fp64"]["value"], 3)
         if mix is not None:
@@ -490,7 +497,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=12)
     ap.add_argument("--in-flight", type=int, default=63, help="steps per ADE launch (1..63)")
     ap.add_argument("--mix-in-flight", type=int, default=31,
-                    help="steps in flight of the ensemble members (memory: slot planes per step)")
+                    help="steps in flight of the FP64 ensemble members (memory: slot planes per step)")
     ap.add_argument("--precision", default="both", choices=("both", "fp64", "fp32"),
                     help="both: FP32 headline with FP64 beside it and the FP32 error")
     ap.add_argument("--no-mix", action="store_true")

@@ -299,7 +299,7 @@ int fx_batch_autotune(fx_batch* b, int trial_steps, int* tile_rows, int* steps_i
   b->dirty = true;
   int best_k = std::min(b->k_limit, kmax);
   best = -1;
-  for (int k : {2, 4, 8, 16, 31}) {
+  for (int k : {2, 4, 8, 16, 31, 63}) {
     if (k > kmax) continue;
     b->k_limit = k;
     b->dirty = true;

@@ -181,7 +181,8 @@ void* fx_batch_stream(fx_batch* b);
  * 1..63; the members' own steps_in_flight bound it too). */
 int fx_batch_set_option(fx_batch* b, const char* name, long long value);
 /* Autotuner of the batch: tries each tile shape, then each steps-in-flight
- * bound, for trial_steps real steps of all members, keeps the fastest
+ * bound (2, 4, 8, 16, 31, 63, up to the members' own), for trial_steps real
+ * steps of all members, keeps the fastest
  * (cell-steps per second) and returns the choice (pointers may be NULL). */
 int fx_batch_autotune(fx_batch* b, int trial_steps, int* tile_rows, int* steps_in_flight);
 
