@@ -29,7 +29,7 @@ FIELDS = ("z", "zb", "h", "qx", "qy", "twet", "h0", "fe_1", "fe_2", "fe_3", "fn_
 # C header symbols, in declaration order (checked by tests/test_capi.py).
 EXPORTED = ("fx_create", "fx_destroy", "fx_last_error", "fx_device_bytes", "fx_footprint", "fx_upload",
             "fx_download",
-            "fx_upload_flags", "fx_download_flags", "fx_set_forcing", "fx_set_manning",
+            "fx_upload_flags", "fx_download_flags", "fx_set_forcing", "fx_set_inflow", "fx_set_manning",
             "fx_set_melt_field", "fx_set_option", "fx_prepare", "fx_step", "fx_run_to_print",
             "fx_print_done", "fx_get_status", "fx_stream", "fx_time_steps", "fx_mass", "fx_autotune",
             "fx_batch_create",
@@ -96,6 +96,7 @@ def lib() -> C.CDLL:
     L.fx_upload_flags.argtypes = [vp, fp, fp]
     L.fx_download_flags.argtypes = [vp, fp, fp, fp]
     L.fx_set_forcing.argtypes = [vp, fp, ip]
+    L.fx_set_inflow.argtypes = [vp, fp, ip, ip]
     L.fx_set_manning.argtypes = [vp, dp]
     L.fx_set_melt_field.argtypes = [vp, dp]
     L.fx_set_option.argtypes = [vp, cp, C.c_longlong]
@@ -298,6 +299,16 @@ class Domain:
         t = np.ascontiguousarray(table, dtype=np.float32)
         assert t.shape == (3, METEO_ROWS)
         self._ck(self.L.fx_set_forcing(self.h, _fptr(t), 1))
+
+    def set_inflow(self, table: Optional[np.ndarray], irow: int = 0, icol: int = 0) -> None:
+        """Point inflow: (3, 2000) float table (time, discharge m^3/s, conc), rows from 0."""
+        if table is None:
+            self._ck(self.L.fx_set_inflow(self.h, None, 0, 0))
+            return
+        t = np.ascontiguousarray(table, dtype=np.float32)
+        assert t.shape == (3, METEO_ROWS)
+        self._keep_inflow = t
+        self._ck(self.L.fx_set_inflow(self.h, _fptr(t), int(irow), int(icol)))
 
     def set_manning(self, grid: Optional[np.ndarray]) -> None:
         self._keep_n = None if grid is None else np.ascontiguousarray(grid, dtype=np.float64)

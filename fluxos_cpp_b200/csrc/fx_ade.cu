@@ -140,6 +140,8 @@ __device__ __forceinline__ T div_area(const fx_dev& d, T x) {
 struct StepIn {
   long long cur;        // slot plane offset of the step
   double meteo_rate, meteoi, mconc, dt;
+  long long inflow_gi;  // the point-inflow cell (-1: none)
+  double inflowi, iconc, inflow_hm;
   bool sweep;           // the sweep runs (hpall != 0 and it > 1)
   bool dilute;          // add_meteo's dilution runs
 };
@@ -216,15 +218,20 @@ __device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, con
     const int ldp = (fl & FX_F_LDRY_PREV) ? 1 : 0;
     T c = R.c[slot][lane][gi & (Ring<T>::CV - 1)];
     const T h0 = R.h0[slot][lane];
+    // the inflow cell holds h0 only after its inflow; the melt's dilution
+    // divides by the depth after the melt (common.cpp:226-234, 313-325)
+    const bool inflow_cell = gi == S.inflow_gi;
+    const T hm = inflow_cell ? (T)S.inflow_hm : h0;
     if (S.dilute && !(fl & FX_F_NODATA)) {
       const T hp = R.hp[slot][lane];
       if (hp != T(0)) {
         const T mi = Fields<T>::mm(d)
                          ? (T)((double)S.meteo_rate * (double)R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
                          : (T)S.meteoi;
-        c = tdiv(c * hp + (mi * (T)S.mconc), h0);
+        c = tdiv(c * hp + (mi * (T)S.mconc), hm);
       }
     }
+    if (inflow_cell && hm != T(0)) c = tdiv(c * hm + (T)(S.inflowi * S.iconc), h0);
     r.c = c;
     if (!S.sweep) r.b = c;
     else if (r.ld == 0 && ldp == 0) r.b = tdiv(c * h0, r.h);
@@ -429,6 +436,10 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
     S.dt = rec.dtfl;
     S.sweep = rec.active && rec.it > 1;  // :45,74-77
     S.dilute = d.has_meteo != 0;
+    S.inflow_gi = d.has_inflow ? d.inflow_gi : -1;
+    S.inflowi = rec.inflowi;
+    S.iconc = rec.iconc;
+    S.inflow_hm = rec.inflow_hm;
     T* A = Fields<T>::conc(d) + k * d.plane;
     const T D = (T)d.dcoef[k];
     const int ix0 = 1 + s * ROWS;

@@ -116,7 +116,7 @@ void fx_fill_status(const fx_ctl& k, fx_status* st) {
   st->finished = k.finished;
   st->device_error = k.error;
   st->forcing_overrun = k.forcing_overrun;
-  st->budget_melt = k.budget_melt;
+  st->budget_melt = k.budget_melt;  // melt and point inflow
   st->budget_out = k.budget_out;
 }
 
@@ -244,6 +244,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
   }
   fx_dev& d = c->d;
   memset(&d, 0, sizeof(d));
+  d.inflow_gi = -1;
   d.nr = g->nrows;
   d.nc = g->ncols;
   d.nchem = g->nchem;
@@ -563,7 +564,46 @@ int fx_set_forcing(fx_ctx* c, const float* tab, int has_meteo) {
   c->d.store_all_fluxes = (c->store_all_opt || c->negative_forcing) ? 1 : 0;
   c->graph_dirty = true;
   c->dev_dirty = true;
-    c->dev_version++;
+  c->dev_version++;
+  return FX_OK;
+}
+
+// The discharge table and cell of add_inflow (common.cpp:277-390). The cell
+// check of common.cpp:324,380-383 (zb equal to NODATA_VALUE) runs once here
+// instead of every step.
+int fx_set_inflow(fx_ctx* c, const float* tab, int irow, int icol) {
+  if (!c) return FX_ERR_ARG;
+  fx_dev& d = c->d;
+  if (!tab) {
+    d.has_inflow = 0;
+    d.inflow_gi = -1;
+  } else {
+    if (irow < 1 || irow > d.nr || icol < 1 || icol > d.nc)
+      return fx_fail(c, FX_ERR_ARG, "fx_set_inflow: cell (%d, %d) is not an interior cell", irow, icol);
+    double zb = 0.0;
+    FX_CK(c, cudaMemcpyAsync(&zb, d.zb + fx_ix(d, irow, icol), sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FX_CK(c, cudaStreamSynchronize(c->stream));
+    if (zb == d.nodata)  // common.cpp:380-383
+      return fx_fail(c, FX_ERR_ARG, "fx_set_inflow: inflow ix,iy in NODATA_VALUE cell");
+    if (!d.inflow_t) {
+      float* t = nullptr;
+      int rc = dev_alloc(c, (void**)&t, sizeof(float) * 3 * FX_METEO_ROWS);
+      if (rc) return rc;
+      d.inflow_t = t;
+      d.inflow_r = t + FX_METEO_ROWS;
+      d.inflow_c = t + 2 * FX_METEO_ROWS;
+    }
+    FX_CK(c, cudaMemcpyAsync((void*)d.inflow_t, tab, sizeof(float) * 3 * FX_METEO_ROWS, cudaMemcpyHostToDevice,
+                             c->stream));
+    FX_CK(c, cudaStreamSynchronize(c->stream));
+    d.has_inflow = 1;
+    d.inflow_irow = irow;
+    d.inflow_icol = icol;
+    d.inflow_gi = fx_ix(d, irow, icol);
+  }
+  c->graph_dirty = true;
+  c->dev_dirty = true;
+  c->dev_version++;
   return FX_OK;
 }
 

@@ -39,6 +39,10 @@ struct fx_steprec {
   int active;         // hpall != 0: the hydrodynamic update and the sweep ran
   int it;             // solver iteration count after the step
   int pad_;
+  double inflowi;     // point-inflow depth added this step (common.cpp:309)
+  double iconc;       // its concentration
+  double inflow_hm;   // depth of the inflow cell after the melt, before the inflow
+                      // (written by the hydrodynamic kernel; the ADE's dilution)
 };
 
 // Step control block, resident in device memory. One thread of k_finalize
@@ -67,11 +71,14 @@ struct fx_ctl {
   int error;             // FX_DEVERR_* set by a kernel
   int pad_;
   long long batch;       // counts launch batches; the ADE sweep takes this batch's steps
-  // water budget since the last reset, FP64 [m^3]: melt added to the cells,
+  // water budget since the last reset, FP64 [m^3]: water added by the
+  // forcing (melt, and the point inflow with its cell's fill to the bed),
   // and water that left through the outflow faces (E face of irow = NROWS,
   // N face of icol = NCOLS)
   double budget_melt;
   double budget_out;
+  double inflowi;     // point-inflow depth of the current step
+  double iconc;       // and its concentration
   fx_steprec rec[FX_MAX_SLOTS];  // per-slot record of the last steps
 };
 
@@ -117,7 +124,13 @@ struct fx_dev {
   const float* meteo_r;
   const float* meteo_c;
   int has_meteo;
-  int pad2_;
+  int has_inflow;     // INFLOW_FILE: a point source at (inflow_irow, inflow_icol)
+  // point-inflow table (float, as GlobVar::inflow; rows from 0) and cell
+  const float* inflow_t;
+  const float* inflow_r;
+  const float* inflow_c;
+  int inflow_irow, inflow_icol;
+  long long inflow_gi;  // fx_ix of the cell, -1 without inflow
   fx_ctl* ctl;
   // Single-precision state (prec32 = 1, fx_hydro.cu hydro_tile32): the depth
   // above the bed eta = z - zb is stored, and the bed enters only through

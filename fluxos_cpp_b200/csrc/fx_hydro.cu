@@ -470,7 +470,7 @@ __device__ __forceinline__ StageOff stage_off(int bx) {
 
 // The fields of the control block a step kernel reads.
 struct StepCtl {
-  double dtfl, meteoi, meteo_rate, mconc;
+  double dtfl, meteoi, meteo_rate, mconc, inflowi;
   long long steps;
   int live, active;
 };
@@ -504,6 +504,29 @@ __device__ __forceinline__ double melt_depth(const fx_dev& d, const StepCtl& c, 
   if (d.melt_mult) return (double)c.meteo_rate * d.melt_mult[gi] / (1000. * 3600. * 24.) * c.dtfl;
   if (d.melt_mult_f) return (double)c.meteo_rate * (double)d.melt_mult_f[gi] / (1000. * 3600. * 24.) * c.dtfl;
   return c.meteoi;
+}
+
+// The point inflow of common.cpp:300-309 on its cell's water level (after
+// the melt): a level below the bed is first raised to the bed, then the
+// step's inflow depth is added.
+__device__ __forceinline__ double inflow_z(double z, double zb, double inflowi) {
+  if (z <= zb) z = zb;
+  return z + inflowi;
+}
+// The same on the FP32 state's compensated depth.
+__device__ __forceinline__ void inflow_eta(float& eta, float& lo, double inflowi) {
+  if (fx_dd_val(eta, lo) <= 0.0) {
+    eta = 0.0f;
+    lo = 0.0f;
+  }
+  fx_dd_add(eta, lo, (float)inflowi);
+}
+__device__ __forceinline__ bool is_inflow(const fx_dev& d, int r, int q) {
+  return d.has_inflow && r == d.inflow_irow && q == d.inflow_icol;
+}
+// The depth the inflow cell had after the melt, for the ADE's dilution.
+__device__ __forceinline__ void record_inflow_hm(const fx_dev& d, const StepCtl& c, double hm) {
+  d.ctl->rec[c.steps % d.nslot].inflow_hm = hm;
 }
 
 
@@ -834,6 +857,15 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         depth = fx_dd_val(eta1, lo1);
         if (depth <= d.hdry) ld = 0;
       }
+      if (is_inflow(d, irow, icol)) {  // common.cpp:300-315
+        const double dm = fx_dd_val(eta1, lo1);
+        record_inflow_hm(d, c, fmax(dm, 0.0));
+        inflow_eta(eta1, lo1, c.inflowi);
+        depth = fx_dd_val(eta1, lo1);
+        bmelt += (depth - dm) * d.arbase;
+        h1 = fmaxf(eta1, 0.0f);
+        ld = depth <= d.hdry ? 1 : 0;
+      }
       const float qx = d.qx_f[pprev + gi], qy = d.qy_f[pprev + gi];
       d.eta[pcur + gi] = eta1;
       d.eta_lo[pcur + gi] = lo1;
@@ -881,6 +913,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         if (melt_on && !(fl & FX_F_NODATA))
           fx_dd_add(eta, lo, (float)(d.melt_mult_f ? (double)c.meteo_rate * (double)g_mm[i4] / (1000. * 3600. * 24.) * c.dtfl
                                                    : c.meteoi));
+        if (is_inflow(d, r, q)) inflow_eta(eta, lo, c.inflowi);
         if (fx_dd_val(eta, lo) <= d.hdry) {
           qx = 0.f;
           qy = 0.f;
@@ -913,6 +946,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         const uint8_t fl = d.flags[sprev + gi];
         if (fl & FX_F_WALL) cl |= C_WALL;
         if (melt_on && !(fl & FX_F_NODATA)) fx_dd_add(eta, lo, (float)melt_depth(d, c, gi));
+        if (is_inflow(d, r, q)) inflow_eta(eta, lo, c.inflowi);
         if (fx_dd_val(eta, lo) <= d.hdry) {
           qx = 0.f;
           qy = 0.f;
@@ -984,13 +1018,22 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     const float eta1 = S.eta[sP];
     const float etapre = stg ? reinterpret_cast<const float*>(stg + L::O_Z)[i4] : d.eta[pprev + gi];
     float h0v = fmaxf(0.0f, etapre);
+    double mi = 0.0;
     if (melt_on && !(fl & FX_F_NODATA)) {
       h0v = fmaxf(eta1, 0.0f);
       if (d.ade) d.hpm_f[scur + gi] = fmaxf(etapre, 0.0f);
-      bmelt = (stg && d.melt_mult_f)
-                  ? (double)c.meteo_rate * (double)reinterpret_cast<const float*>(stg + L::O_MM)[i4] /
-                        (1000. * 3600. * 24.) * c.dtfl * d.arbase
-                  : melt_depth(d, c, gi) * d.arbase;
+      mi = (stg && d.melt_mult_f) ? (double)c.meteo_rate * (double)reinterpret_cast<const float*>(stg + L::O_MM)[i4] /
+                                        (1000. * 3600. * 24.) * c.dtfl
+                                  : melt_depth(d, c, gi);
+      bmelt = mi * d.arbase;
+    }
+    if (is_inflow(d, irow, icol)) {  // common.cpp:300-315 (h0 = the depth after the inflow)
+      float em = etapre, lm = stg ? reinterpret_cast<const float*>(stg + L::O_LO)[i4] : d.eta_lo[pprev + gi];
+      if (melt_on && !(fl & FX_F_NODATA)) fx_dd_add(em, lm, (float)mi);
+      const double dm = fx_dd_val(em, lm);
+      record_inflow_hm(d, c, fmax(dm, 0.0));
+      bmelt += (fx_dd_val(eta1, S.eta_lo[sP]) - dm) * d.arbase;
+      h0v = fmaxf(eta1, 0.0f);
     }
     if (!(cl & C_DRY)) d.twet_f[gi] += (float)(c.dtfl / 3600);
     float dh = 0.f, dqx = 0.f, dqy = 0.f, qxfP = 0.f, qyfP = 0.f;
@@ -1105,6 +1148,14 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
         h1 = fmax(z1 - zb, 0.0);
         if (h1 <= d.hdry) ld = 0;  // common.cpp:219-222
       }
+      if (is_inflow(d, irow, icol)) {  // common.cpp:300-315
+        const double zm = z1;
+        record_inflow_hm(d, c, fmax(zm - zb, 0.0));
+        z1 = inflow_z(z1, zb, c.inflowi);
+        h1 = fmax(z1 - zb, 0.0);
+        ld = h1 <= d.hdry ? 1 : 0;
+        bmelt += (z1 - zm) * d.arbase;
+      }
       const double qx = d.qx[pprev + gi], qy = d.qy[pprev + gi];
       d.z[pcur + gi] = z1;
       d.qx[pcur + gi] = qx;
@@ -1149,6 +1200,7 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
         if (g_fl[sc * STG_W1 + sr + so.o1] & FX_F_WALL) cl |= C_WALL;
         if (melt_on && zb != d.nodata)
           z = z + (d.melt_mult ? (double)c.meteo_rate * g_mm[i8] / (1000. * 3600. * 24.) * c.dtfl : c.meteoi);
+        if (is_inflow(d, r, q)) z = inflow_z(z, zb, c.inflowi);
         const double h1 = fmax(0.0, z - zb);
         if (h1 <= d.hdry) {
           qx = 0.0;
@@ -1178,6 +1230,7 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
         cl = C_INT;
         if (d.flags[sprev + gi] & FX_F_WALL) cl |= C_WALL;
         if (melt_on && zb != d.nodata) z = z + melt_depth(d, c, gi);
+        if (is_inflow(d, r, q)) z = inflow_z(z, zb, c.inflowi);
         const double h1 = fmax(0.0, z - zb);
         if (h1 <= d.hdry) {
           qx = 0.0;
@@ -1265,13 +1318,20 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     // Courant scan's copy of h (main.cpp:305) for cells it skips. Its solute
     // dilution (:226-234) is applied by the ADE sweep (fx_ade.cu).
     double h0v = fmax(0.0, zpre - zb);
+    double mi = 0.0;
     if (melt_on && zb != d.nodata) {
       h0v = fmax(z1 - zb, 0.0);
       if (d.ade) d.hpm[scur + gi] = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
-      bmelt = (stg && d.melt_mult)
-                  ? (double)c.meteo_rate * reinterpret_cast<const double*>(stg + L::O_MM)[i8] /
-                        (1000. * 3600. * 24.) * c.dtfl * d.arbase
-                  : melt_depth(d, c, gi) * d.arbase;
+      mi = (stg && d.melt_mult) ? (double)c.meteo_rate * reinterpret_cast<const double*>(stg + L::O_MM)[i8] /
+                                      (1000. * 3600. * 24.) * c.dtfl
+                                : melt_depth(d, c, gi);
+      bmelt = mi * d.arbase;
+    }
+    if (is_inflow(d, irow, icol)) {  // common.cpp:300-315 (h0 = the depth after the inflow)
+      const double zm = (melt_on && zb != d.nodata) ? zpre + mi : zpre;
+      record_inflow_hm(d, c, fmax(zm - zb, 0.0));
+      bmelt += (z1 - zm) * d.arbase;
+      h0v = fmax(z1 - zb, 0.0);
     }
     // Loop 1 wet time (:69-70)
     if (!(cl & C_DRY)) d.twet[gi] += dtl / 3600;
@@ -1372,6 +1432,7 @@ __device__ __forceinline__ void hydro_block(const fx_dev& d, const fx_tile& tile
     sc.meteoi = g.meteoi;
     sc.meteo_rate = g.meteo_rate;
     sc.mconc = g.mconc;
+    sc.inflowi = g.inflowi;
     sc.steps = g.steps;
     sc.live = g.live;
     sc.active = g.active;
@@ -1502,6 +1563,7 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
     sc.meteoi = g.meteoi;
     sc.meteo_rate = g.meteo_rate;
     sc.mconc = g.mconc;
+    sc.inflowi = g.inflowi;
     sc.steps = g.steps;
     sc.live = g.live;
     sc.active = g.active;
@@ -1630,6 +1692,18 @@ __global__ void k_finalize(const fx_dev* __restrict__ devs, int ndom) {
     c.meteoi = 0.0;
     c.mconc = 0.0;
   }
+  if (d.has_inflow) {  // common.cpp:300-311; table rows from 0 (read_functions.cpp:311)
+    int row = forcing_row(d.inflow_t, c.tim);
+    if (row < 0) {
+      c.forcing_overrun = 1;
+      row = FX_METEO_ROWS - 1;
+    }
+    c.inflowi = (double)d.inflow_r[row] * dt / d.arbase;  // / pow(dxy, 2), exact
+    c.iconc = (double)d.inflow_c[row];
+  } else {
+    c.inflowi = 0.0;
+    c.iconc = 0.0;
+  }
   c.active = hpall != 0.0;
   if (c.active) c.it = c.it + 1;
   c.print_pending = c.tim >= c.print_next;
@@ -1639,6 +1713,9 @@ __global__ void k_finalize(const fx_dev* __restrict__ devs, int ndom) {
   r.meteoi = c.meteoi;
   r.meteo_rate = c.meteo_rate;
   r.mconc = c.mconc;
+  r.inflowi = c.inflowi;
+  r.iconc = c.iconc;
+  r.inflow_hm = 0.0;
   r.step = c.steps;
   r.batch = c.batch;
   r.live = 1;

@@ -218,9 +218,10 @@ bool first_double(const std::string& line, double* out) {
 }
 
 struct Modset {
-  std::string dem_file, meteo_file, output_folder;
+  std::string dem_file, meteo_file, inflow_file, output_folder;
   bool restart = false, ade = false, has_meteo = false, has_inflow = false;
   unsigned long print_step = 0, h_min_print = 0;
+  unsigned long inflow_x = 0, inflow_y = 0;  // DISCHARGE_LOCATION (GlobVar.h:100)
   double ks = 0.0, d_coef = 0.0;
 };
 
@@ -283,14 +284,22 @@ int read_modset(const std::string& path, Modset& m, std::string& err) {
     m.meteo_file = v->s;
     m.has_meteo = !m.meteo_file.empty();
   }
-  m.has_inflow = root.get("INFLOW_FILE") != nullptr;
+  // INFLOW_FILE.FILENAME and DISCHARGE_LOCATION (read_functions.cpp:74-88)
+  if (const JVal* inf = root.get("INFLOW_FILE")) {
+    m.has_inflow = true;
+    const JVal* fn = inf->get("FILENAME");
+    const JVal* loc = inf->get("DISCHARGE_LOCATION");
+    if (!fn || fn->kind != JVal::STR || !loc) {
+      err = "modset: INFLOW_FILE needs FILENAME and DISCHARGE_LOCATION";
+      return FX_ERR_IO;
+    }
+    m.inflow_file = fn->s;
+    m.inflow_x = as_ulong(loc->get("X_COORDINATE"));
+    m.inflow_y = as_ulong(loc->get("Y_COORDINATE"));
+  }
   if (!m.has_meteo && !m.has_inflow) {
     err = "METEO_FILE or INFLOW_FILE must be provided in master file: " + path;
     return FX_ERR_IO;
-  }
-  if (m.has_inflow) {
-    err = "INFLOW_FILE (point inflow) is not supported by this build";
-    return FX_ERR_ARG;
   }
   return FX_OK;
 }
@@ -385,6 +394,50 @@ std::vector<std::vector<double>> read_csv_numbers(const std::string& path, bool*
     rows.push_back(r);
   }
   return rows;
+}
+
+// read_inflow (read_functions.cpp:284-326): data row a (1-based after the
+// header) goes to table row a - 1, columns t [s], discharge [m^3/s],
+// concentration, stored as float. `tlast` is the last data row's time, the
+// value read_inflow returns for ntim.
+int read_inflow_table(const Modset& m, std::vector<float>& tab, double* tlast, std::string& err) {
+  tab.assign(3 * (size_t)FX_METEO_ROWS, 0.0f);
+  *tlast = 0.0;
+  bool ok = false;
+  auto rows = read_csv_numbers(m.inflow_file, &ok);
+  if (!ok) {
+    err = "cannot open INFLOW_FILE " + m.inflow_file;
+    return FX_ERR_IO;
+  }
+  if (rows.size() > (size_t)FX_METEO_ROWS + 1) {
+    err = "INFLOW_FILE has more than " + std::to_string(FX_METEO_ROWS) + " rows";
+    return FX_ERR_ARG;
+  }
+  for (size_t a = 1; a < rows.size(); ++a) {
+    for (int col = 0; col < 3; ++col)
+      tab[(size_t)col * FX_METEO_ROWS + a - 1] = (float)(col < (int)rows[a].size() ? rows[a][col] : 0.0);
+    *tlast = rows[a].empty() ? 0.0 : rows[a][0];
+  }
+  return FX_OK;
+}
+
+// read_geo's discharge cell (read_functions.cpp:228-231): round(coordinate -
+// corner) / dxy, truncated into an unsigned long. The reference leaves the
+// cell unset when both coordinates are 0 and indexes outside the grid for a
+// location off the DEM; both are refused here.
+int inflow_cell(const Modset& m, double xll, double yll, int dxy, int nrows, int ncols, int* irow,
+                int* icol, std::string& err) {
+  const double r = std::round((double)m.inflow_y - yll) / (double)dxy;
+  const double q = std::round((double)m.inflow_x - xll) / (double)dxy;
+  if ((m.inflow_x == 0 && m.inflow_y == 0) || !(r >= 1.0) || !(q >= 1.0) || r >= nrows + 1.0 ||
+      q >= ncols + 1.0) {
+    err = "INFLOW_FILE: DISCHARGE_LOCATION (" + std::to_string(m.inflow_x) + ", " +
+          std::to_string(m.inflow_y) + ") is not an interior cell of the DEM";
+    return FX_ERR_ARG;
+  }
+  *irow = (int)(unsigned long)r;
+  *icol = (int)(unsigned long)q;
+  return FX_OK;
 }
 
 // read_geo's wall / ks step (read_functions.cpp:175-225) and initiation's
@@ -618,7 +671,17 @@ int fx_load_modset(const char* modset_path, fx_grid* g_out, fx_params* p_out, do
   fx_params p{};
   p.hdry = m.ks;  // ks(1,1) (main.cpp:259)
   p.ks = m.ks;
-  p.ntim = (double)(int)(float)tlast;  // float read_meteo -> int (main.cpp:74,181,192)
+  int ntim = (int)(float)tlast;  // float read_meteo -> int (main.cpp:74,181)
+  if (m.has_inflow) {  // ntim = max(ntim_meteo, ntim_inflow) (main.cpp:184-192)
+    std::vector<float> itab;
+    double tin = 0.0;
+    int irow = 0, icol = 0;
+    if ((rc = read_inflow_table(m, itab, &tin, err)) ||
+        (rc = inflow_cell(m, dm.xll, dm.yll, dm.dxy, dm.nrows, dm.ncols, &irow, &icol, err)))
+      return fx_fail(nullptr, rc, "%s", err.c_str());
+    ntim = std::max(ntim, (int)(float)tin);
+  }
+  p.ntim = (double)ntim;
   p.print_step = (double)m.print_step;
   p.h_min_print = (double)m.h_min_print;
   p.ade = m.ade ? 1 : 0;
@@ -701,7 +764,27 @@ int fx_open_modset(const char* modset_path, fx_ctx** out) {
       (rc = fx_upload(c, "h", h.data())) || (rc = fx_upload(c, "qx", qx.data())) ||
       (rc = fx_upload(c, "qy", qy.data())) || (rc = fx_upload(c, "twet", tw.data())) ||
       (rc = fx_upload(c, "conc", cc.data())) || (rc = fx_upload_flags(c, ldry.data(), wall.data())) ||
-      (rc = fx_set_forcing(c, tab.data(), has_meteo)) || (rc = fx_prepare(c))) {
+      (rc = fx_set_forcing(c, tab.data(), has_meteo))) {
+    std::string e = c->err;
+    fx_destroy(c);
+    return fx_fail(nullptr, rc, "%s", e.c_str());
+  }
+  if (m.has_inflow) {
+    std::vector<float> itab;
+    double tin = 0.0;
+    int irow = 0, icol = 0;
+    if ((rc = read_inflow_table(m, itab, &tin, err)) ||
+        (rc = inflow_cell(m, g.xll, g.yll, g.dxy, g.nrows, g.ncols, &irow, &icol, err))) {
+      fx_destroy(c);
+      return fx_fail(nullptr, rc, "%s", err.c_str());
+    }
+    if ((rc = fx_set_inflow(c, itab.data(), irow, icol))) {
+      std::string e = c->err;
+      fx_destroy(c);
+      return fx_fail(nullptr, rc, "%s", e.c_str());
+    }
+  }
+  if ((rc = fx_prepare(c))) {
     std::string e = c->err;
     fx_destroy(c);
     return fx_fail(nullptr, rc, "%s", e.c_str());

@@ -9,7 +9,11 @@ drive the reference program and this package:
   (``common.cpp:110-161``, ``read_functions.cpp:112-235``). The first data
   line is grid row ``irow = NROWS`` (``read_functions.cpp:145-163``);
 * ``meteo.csv``: header plus ``time [s], rate [mm/day], concentration`` rows
-  read by ``read_meteo`` (``read_functions.cpp:237-282``).
+  read by ``read_meteo`` (``read_functions.cpp:237-282``);
+* ``inflow.csv`` (only with a point inflow): header plus ``time [s],
+  discharge [m^3/s], concentration`` rows read by ``read_inflow``
+  (``read_functions.cpp:284-326``), entering the cell of the modset's
+  ``INFLOW_FILE.DISCHARGE_LOCATION``.
 
 The reference picks the first forcing row whose time exceeds the clock
 (``common.cpp:195-200``) and sets the run length from the last row's time
@@ -57,6 +61,11 @@ class Scenario:
     manning: Optional[np.ndarray] = None
     melt_mult: Optional[np.ndarray] = None
     d_coefs: Optional[List[float]] = None  # one D per solute (>= 1 solutes)
+    # Optional point inflow (INFLOW_FILE): rows (t [s], discharge [m^3/s],
+    # concentration) and the discharge location (X, Y) in the DEM's
+    # coordinates, integers as the reference stores them (GlobVar.h:100).
+    inflow: Optional[Sequence[Tuple[float, float, float]]] = None
+    inflow_xy: Optional[Tuple[int, int]] = None
     # Optional wet start (interior arrays, same shape as dem).
     init_h: Optional[np.ndarray] = None
     init_qx: Optional[np.ndarray] = None
@@ -84,6 +93,9 @@ class Scenario:
         out_dir = os.path.join(folder, "Results")
         write_esri_ascii(dem_path, self.dem, self.dxy, self.xll, self.yll, self.nodata)
         write_meteo(met_path, self.meteo, self.horizon)
+        inflow_path = os.path.join(folder, "inflow.csv")
+        if self.inflow is not None:
+            write_meteo(inflow_path, self.inflow, self.horizon)
         modset = {
             "COMMNET": f"synthetic scenario {self.name}",
             "DEM_FILE": dem_path,
@@ -104,6 +116,10 @@ class Scenario:
                 "WINTRA": {"STATUS": False, "SWE_STD": 0.0, "SWE_MAX": 0.0},
             },
         }
+        if self.inflow is not None:
+            x, y = self.inflow_xy
+            modset["INFLOW_FILE"] = {"FILENAME": inflow_path,
+                                     "DISCHARGE_LOCATION": {"X_COORDINATE": int(x), "Y_COORDINATE": int(y)}}
         path = os.path.join(folder, "modset.json")
         with open(path, "w") as f:
             f.write("// FLUXOS master file (comments allowed, main.cpp:106-109)\n")
@@ -287,6 +303,27 @@ def forcing_table(sc: Scenario) -> np.ndarray:
     return tab
 
 
+def inflow_table(sc: Scenario) -> np.ndarray:
+    """The point-inflow table as read_inflow fills GlobVar::inflow (3 x 2000
+    float, data from row 0, read_functions.cpp:307-313), with the guard and
+    horizon rows of write_meteo."""
+    tab = np.zeros((3, 2000), dtype=np.float32)
+    rows = list(sc.inflow) + [(GUARD_TIME, 0.0, 0.0), (sc.horizon, 0.0, 0.0)]
+    for a, (t, r, c) in enumerate(rows):
+        tab[:, a] = (t, r, c)
+    return tab
+
+
+def inflow_cell(sc: Scenario) -> Tuple[int, int]:
+    """(irow, icol) of the discharge location as read_geo computes it
+    (read_functions.cpp:228-231): round(coordinate - corner) / dxy, stored in
+    an unsigned long."""
+    x, y = sc.inflow_xy
+    irow = int(math.floor(round(float(int(y)) - float(sc.yll)) / float(sc.dxy)))
+    icol = int(math.floor(round(float(int(x)) - float(sc.xll)) / float(sc.dxy)))
+    return irow, icol
+
+
 def full_grid(sc: Scenario, interior: np.ndarray, fill: float = 0.0) -> np.ndarray:
     """An interior (nrows, ncols) array as a GlobVar grid (ncols+2, nrows+2)."""
     g = np.full((sc.ncols + 2, sc.nrows + 2), fill)
@@ -305,6 +342,8 @@ def make_domain(sc: Scenario, *, precision: str = "fp64", steps_in_flight: int =
                   steps_in_flight=steps_in_flight, precision=precision)
     d.initiate(full_grid(sc, sc.dem.astype(np.float64)))
     d.set_forcing(forcing_table(sc))
+    if sc.inflow is not None:
+        d.set_inflow(inflow_table(sc), *inflow_cell(sc))
     if sc.melt_mult is not None:
         d.set_melt_field(full_grid(sc, sc.melt_mult, 1.0))
     if sc.manning is not None:

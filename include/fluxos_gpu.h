@@ -85,7 +85,7 @@ typedef struct fx_status {
   int finished;         /* tim > ntim: the run is over */
   int device_error;     /* nonzero when a kernel gave up a bounded wait */
   int forcing_overrun;  /* the forcing table had no row later than tim */
-  double budget_melt;   /* water added by the forcing since creation [m^3], FP64 */
+  double budget_melt;   /* water added by the forcing (melt, point inflow) since creation [m^3], FP64 */
   double budget_out;    /* water that left through the outflow faces (E face of
                            irow = NROWS, N face of icol = NCOLS) or into wall
                            cells since creation [m^3], FP64 */
@@ -115,6 +115,15 @@ int fx_download_flags(fx_ctx* ctx, float* ldry, float* ldry_prev, float* wall);
  * [mm/day], concentration), column-major float as arma::fmat(2000,3).
  * has_meteo = 0 means no METEO_FILE (add_meteo returns at common.cpp:190). */
 int fx_set_forcing(fx_ctx* ctx, const float* table_2000x3, int has_meteo);
+/* Point inflow of INFLOW_FILE (add_inflow, common.cpp:277-390): the table of
+ * GlobVar::inflow, 2000 rows x 3 columns (time [s], discharge [m^3/s],
+ * concentration) column-major float with data from row 0, and the interior
+ * cell (irow, icol) it enters (read_functions.cpp:228-231). NULL switches it
+ * off. FX_ERR_ARG if the cell is outside the interior or a NODATA cell. With
+ * more than one solute every solute takes the table's one concentration
+ * column (the reference's table has one). The discharged volume is counted
+ * in fx_status.budget_melt. */
+int fx_set_inflow(fx_ctx* ctx, const float* table_2000x3, int irow, int icol);
 /* Extensions without a reference counterpart (NULL switches them off):
  * per-cell Manning n (semi-implicit friction after the update) and a
  * per-cell multiplier of the melt rate. Full grids as for fx_upload. */

@@ -126,6 +126,16 @@ def read_meteo_table(path: str) -> np.ndarray:
     return tab
 
 
+def read_inflow_table(path: str) -> np.ndarray:
+    """The 2000x3 float point-inflow table as read_inflow fills it
+    (read_functions.cpp:303-316): like the forcing table, but data row k
+    (1-based after the header) into table row k - 1."""
+    tab = read_meteo_table(path)
+    out = np.zeros_like(tab)
+    out[:, :-1] = tab[:, 1:]
+    return out
+
+
 class _Run:
     nrows: int
     ncols: int
@@ -187,7 +197,18 @@ class OracleRun(_Run):
         L.ox_set_scalar(s, b"has_meteo", 1.0)
         n_data = self._meteo_rows(os.path.join(modset_dir, "meteo.csv"))
         last_t = float(tab[0, n_data]) if n_data > 0 else 0.0
-        L.ox_set_scalar(s, b"ntim", float(int(np.float32(last_t))))  # main.cpp:181-192
+        ntim = int(np.float32(last_t))
+        if sc.inflow is not None:  # read_inflow, read_geo's discharge cell (read_functions.cpp:228-231)
+            from fluxos_cpp_b200 import scenarios as _S
+            itab = read_inflow_table(os.path.join(modset_dir, "inflow.csv"))
+            self.fgrid("inflow")[...] = itab
+            L.ox_set_scalar(s, b"has_inflow", 1.0)
+            irow, icol = _S.inflow_cell(sc)
+            L.ox_set_scalar(s, b"inflow_nrow", float(irow))
+            L.ox_set_scalar(s, b"inflow_ncol", float(icol))
+            n_in = self._meteo_rows(os.path.join(modset_dir, "inflow.csv"))
+            ntim = max(ntim, int(np.float32(itab[0, n_in - 1])) if n_in > 0 else 0)
+        L.ox_set_scalar(s, b"ntim", float(ntim))  # main.cpp:181-192
         L.ox_set_scalar(s, b"print_next", float(sc.print_step))
         self._keep = []
         if sc.manning is not None:

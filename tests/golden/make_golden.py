@@ -2,12 +2,12 @@
 
 Run from the repository root where the reference tree is mounted:
 
-    make -C oracle all && python tests/golden/make_golden.py
+    make -C oracle all && python tests/golden/make_golden.py [case ...]
 
 Each case is a small seeded scenario. Its input files are written exactly as
 the reference reads them, and the reference sources compiled in
 oracle/_ref/ are stepped through the harness (oracle/ref_harness.cpp). State
-snapshots are saved at the listed step counts. One case also keeps the
+snapshots are saved at the listed step counts. Two cases also keep the
 Results/<t>.txt files that the whole reference program (oracle/_ref/fluxos_ref)
 writes. The fixtures hold the input text, so tests need neither the reference
 nor this script.
@@ -72,11 +72,24 @@ def case_dambreak() -> dict:
                 steps=(1, 20, 200), mode=0, results=False)
 
 
+def case_inflow() -> dict:
+    """A point inflow (INFLOW_FILE) on a dry plane under melt: three discharge
+    rows with their own concentrations, then none."""
+    sc = S.plane_scenario(24, 20, seed=2)
+    sc.horizon = 4000.0
+    sc.meteo = ((0.0, 20.0, 1.0), (4000.0, 20.0, 1.0))
+    sc.inflow = ((0.0, 0.02, 5.0), (300.0, 0.05, 2.0), (900.0, 0.01, 0.5), (1500.0, 0.0, 0.0))
+    sc.inflow_xy = (24, 32)  # icol 12, irow 16 at dxy 2
+    sc.dem[8, 3:9] = -9999.0
+    return dict(sc=sc, wet=None, steps=(1, 10, 200, 2000), mode=0, results=True)
+
+
 CASES = {
     "plane_walls": case_plane_walls,
     "patchwork_weir": lambda: case_patchwork(0),
     "patchwork_closed": lambda: case_patchwork(1),
     "dambreak": case_dambreak,
+    "inflow": case_inflow,
 }
 
 
@@ -93,6 +106,11 @@ def build_case(name: str, spec: dict) -> None:
                 print_step=sc.print_step, ks=sc.ks, ade=sc.ade, d_coef=sc.d_coef,
                 h_min_print=sc.h_min_print, volrat_mode=mode, steps=list(spec["steps"]),
                 wet=spec["wet"] is not None)
+    if sc.inflow is not None:
+        with open(os.path.join(work, "inflow.csv")) as f:
+            out["inflow_csv"] = np.array(f.read())
+        meta["inflow"] = [list(r) for r in sc.inflow]
+        meta["inflow_xy"] = list(sc.inflow_xy)
     ref = P.RefRun(modset, sc, mode)
     if spec["wet"] is not None:
         w = spec["wet"]
@@ -132,8 +150,10 @@ def build_case(name: str, spec: dict) -> None:
 def main() -> None:
     if not P.ref_available(0):
         sys.exit("oracle/_ref is not built: run `make -C oracle all` with the reference present")
+    only = set(sys.argv[1:])
     for name, fn in CASES.items():
-        build_case(name, fn())
+        if not only or name in only:
+            build_case(name, fn())
 
 
 if __name__ == "__main__":

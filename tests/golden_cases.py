@@ -7,7 +7,7 @@ import numpy as np
 from fluxos_cpp_b200 import scenarios as S
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ("plane_walls", "patchwork_weir", "patchwork_closed", "dambreak")
+CASES = ("plane_walls", "patchwork_weir", "patchwork_closed", "dambreak", "inflow")
 
 
 def load(name: str):
@@ -38,6 +38,14 @@ def materialise(name: str, folder: str):
                              "OPENWQ": {"STATUS": False, "MASTERFILE_DIR": ""},
                              "WINTRA": {"STATUS": False, "SWE_STD": 0.0, "SWE_MAX": 0.0}},
     }
+    if "inflow_csv" in z.files:
+        with open(os.path.join(folder, "inflow.csv"), "w") as f:
+            f.write(str(z["inflow_csv"]))
+        sc.inflow = [tuple(r) for r in meta["inflow"]]
+        sc.inflow_xy = tuple(meta["inflow_xy"])
+        modset["INFLOW_FILE"] = {"FILENAME": os.path.join(folder, "inflow.csv"),
+                                 "DISCHARGE_LOCATION": {"X_COORDINATE": sc.inflow_xy[0],
+                                                        "Y_COORDINATE": sc.inflow_xy[1]}}
     mp = os.path.join(folder, "modset.json")
     with open(mp, "w") as f:
         f.write("/* golden case */\n")

@@ -23,6 +23,8 @@ def domain_from_oracle(ora, sc, volrat_mode=0, store_all=True, steps_in_flight=0
         d.upload(nm, ora.grid(nm))
     d.upload_flags(ora.grid("ldry"), ora.grid("wall"))
     d.set_forcing(ora.fgrid("meteo"))
+    if ora.scalar("has_inflow"):
+        d.set_inflow(ora.fgrid("inflow"), int(ora.scalar("inflow_nrow")), int(ora.scalar("inflow_ncol")))
     if sc.manning is not None:
         m = np.zeros(d.shape)
         m[1:-1, 1:-1] = sc.manning.T

@@ -117,6 +117,37 @@ def test_fp32_dambreak():
     _check("dambreak256", sc, 1, short=[2.0, 5.0], long_=[10.0, 20.0])
 
 
+def test_fp32_point_inflow():
+    """A point inflow (add_inflow) into the fractal scenario adds no FP32
+    error of its own: at equal times the FP32 depth error with the inflow
+    stays that of the same scenario without it, below 1e-4 on the short
+    horizons, and both precisions close their water balance with the
+    discharged volume counted in the budget."""
+    base = _fractal(192)
+    sc = _fractal(192)
+    sc.inflow = ((0.0, 0.0, 0.0), (60.0, 0.2, 2.0), (120.0, 0.05, 1.0))  # 0.2 m^3/s, then 0.05
+    sc.inflow_xy = (2 * 100, 2 * 90)
+    base.print_step = sc.print_step = 5
+    d64, d32 = S.make_domain(sc, precision="fp64"), S.make_domain(sc, precision="fp32")
+    e64, e32 = S.make_domain(base, precision="fp64"), S.make_domain(base, precision="fp32")
+    w64, w32 = d64.mass()[0], d32.mass()[0]
+    for t in (5.0, 20.0, 60.0, 120.0):
+        for d in (d64, d32, e64, e32):
+            _run_to(d, t)
+        l1 = A.state_errors(d32, d64, sc.ks)["depth"]["l1_rel"]
+        l1b = A.state_errors(e32, e64, sc.ks)["depth"]["l1_rel"]
+        print("inflow192", t, "fp32 L1 with inflow %.3e without %.3e" % (l1, l1b))
+        if t <= 20.0:
+            assert l1 <= L1_DEPTH_TOL, (t, l1)
+        assert l1 <= 1.5 * l1b + 1e-6, (t, l1, l1b)
+    for k in ("h", "qx", "qy", "conc"):
+        assert np.all(np.isfinite(d32.download(k))), k
+    b64, b32 = A.water_balance(d64, w64), A.water_balance(d32, w32)
+    assert b64["rel_err"] <= MASS_TOL and b32["rel_err"] <= MASS_TOL, (b64, b32)
+    assert b64["melt_in"] > 0.2 * 60.0 + 0.05 * 60.0
+    assert abs(b32["melt_in"] - b64["melt_in"]) <= 1e-3 * b64["melt_in"]
+
+
 def test_fp32_state_stays_finite():
     """The large-domain workload's wet start (5 mm film plus ponded
     depressions) on steep fractal terrain: FP32 Ritter inflows whose surface
@@ -161,6 +192,8 @@ def test_fp32_z_surface_and_upload_order():
 
 def test_fp32_batch_bit_identical_to_alone():
     scs = [_fractal(n) for n in (64, 150)]
+    scs[1].inflow = ((0.0, 0.0, 0.0), (1e4, 0.1, 2.0))
+    scs[1].inflow_xy = (2 * 70, 2 * 40)
     batched = [S.make_domain(sc, precision="fp32", steps_in_flight=4) for sc in scs]
     alone = [S.make_domain(sc, precision="fp32", steps_in_flight=4) for sc in scs]
     b = fx.Batch()

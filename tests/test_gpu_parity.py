@@ -163,3 +163,35 @@ def test_extensions_multi_solute_manning_melt_field(tmp_path):
         res, bad = GP.compare(ora, d, sc, rtol=1e-9)
         assert not bad, (n, bad)
     d.close()
+
+
+@pytest.mark.parametrize("tma,in_flight,cell", [(1, 8, (90, 70)), (0, 1, (90, 70)), (1, 31, (1, 1)),
+                                                (0, 3, (150, 130))])
+def test_point_inflow_parity(tma, in_flight, cell, tmp_path):
+    """Point inflow (INFLOW_FILE, add_inflow) on a wet patchwork large enough
+    for the TMA-staged kernel. A row applies until its own time (the first
+    row later than the clock, common.cpp:306-312), so the discharge starts at
+    40 s, changes rate and concentration at 80 s and stops at 150 s; the
+    inflow cell sits inside the grid or in a corner."""
+    nr, nc = 150, 130
+    sc = _random_scenario(nr, nc, 41)
+    irow, icol = cell
+    plain = S.plane_scenario(nr, nc, seed=41).dem
+    sc.dem[nr - irow, icol - 1] = plain[nr - irow, icol - 1]  # not a wall
+    sc.inflow = ((0.0, 0.05, 4.0), (40.0, 0.0, 0.0), (80.0, 0.02, 1.0), (150.0, 0.08, 0.0))
+    sc.inflow_xy = (icol * sc.dxy, irow * sc.dxy)
+    sc.write(str(tmp_path))
+    ora = P.OracleRun(str(tmp_path), sc, 0)
+    assert S.inflow_cell(sc) == cell
+    rng = np.random.default_rng(5)
+    h = np.where(rng.random((nr, nc)) < 0.5, rng.uniform(0, 0.03, (nr, nc)), 0.0)
+    ora.apply_wet_start(h, None, None, [np.where(h > 0.01, 1.0, 0.0)])
+    d = GP.domain_from_oracle(ora, sc, 0, steps_in_flight=in_flight)
+    d.set_option("tma", tma)
+    for n in (1, 20, 150, 400, 500):
+        GP.advance_oracle(ora, n)
+        GP.advance_domain(d, n)
+        res, bad = GP.compare(ora, d, sc)
+        assert not bad, (n, bad)
+    assert ora.scalar("tim") > 150.0  # every discharge row was used
+    d.close()

@@ -1,7 +1,7 @@
 """The drop-in surface on the GPU: `fluxos_gpu <modset.json>` (and the
 library's fx_open_modset / fx_run_to_print / fx_write_results behind it)
 against the Results files the reference program wrote for the same inputs
-(tests/golden/plane_walls.npz, frozen from the reference).
+(tests/golden/plane_walls.npz and inflow.npz, frozen from the reference).
 
 Every file must list the same cells in the same order with the same
 integer and coordinate columns; state columns agree within 1e-10 relative
@@ -40,8 +40,9 @@ def _compare_results(folder, z, meta):
             assert float(err.max()) <= 1e-10, (fn, col, float(err.max()))
 
 
-def test_program_matches_reference_results(tmp_path):
-    sc, z, meta, mp = G.materialise("plane_walls", str(tmp_path))
+@pytest.mark.parametrize("case", ["plane_walls", "inflow"])
+def test_program_matches_reference_results(case, tmp_path):
+    sc, z, meta, mp = G.materialise(case, str(tmp_path))
     r = subprocess.run([fx.EXE_PATH, mp], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     _compare_results(os.path.join(str(tmp_path), "Results"), z, meta)

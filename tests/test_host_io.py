@@ -57,6 +57,44 @@ def test_missing_forcing_is_an_error(tmp_path):
     assert "METEO_FILE or INFLOW_FILE" in str(e.value)
 
 
+def _inflow_modset(tmp_path, xy, meteo=True, horizon=3000.0):
+    sc = S.plane_scenario(12, 10)
+    sc.horizon = horizon
+    sc.inflow = ((0.0, 0.01, 1.0), (1200.0, 0.0, 0.0))
+    sc.inflow_xy = xy
+    mp = sc.write(str(tmp_path))
+    if not meteo:
+        m = json.loads(open(mp).read().split("\n", 1)[1])
+        del m["METEO_FILE"]
+        open(mp, "w").write(json.dumps(m))
+    return sc, mp
+
+
+def test_inflow_only_modset_takes_ntim_from_the_inflow_file(tmp_path):
+    """INFLOW_FILE alone is enough (read_functions.cpp:74-95); ntim is the
+    inflow file's last time as read_inflow returns it (main.cpp:184-192)."""
+    sc, mp = _inflow_modset(tmp_path, (4, 6), meteo=False, horizon=2500.5)
+    st = fx.load_modset(mp)
+    assert st["has_meteo"] == 0
+    assert st["params"]["ntim"] == 2500.0
+    assert not st["meteo"].any()
+    if P.ref_available(0):
+        ref = P.RefRun(mp, sc, 0)
+        assert ref.scalar("ntim") == st["params"]["ntim"]
+        assert ref.scalar("has_inflow") == 1.0
+        assert (ref.scalar("inflow_nrow"), ref.scalar("inflow_ncol")) == S.inflow_cell(sc) == (3, 2)
+
+
+@pytest.mark.parametrize("xy", [(0, 0), (4, 60), (40, 6), (4, 1)])
+def test_inflow_location_off_the_interior_is_an_error(xy, tmp_path):
+    """Both coordinates 0 leave the reference's cell unset, and a cell off
+    the DEM's interior would be indexed outside the grid: both refused."""
+    _, mp = _inflow_modset(tmp_path, xy)
+    with pytest.raises(fx.FluxosError) as e:
+        fx.load_modset(mp)
+    assert "DISCHARGE_LOCATION" in str(e.value)
+
+
 def test_restart_reads_newest_results_file(tmp_path):
     sc = S.plane_scenario(8, 7)
     mp = sc.write(str(tmp_path))

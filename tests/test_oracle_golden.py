@@ -36,11 +36,12 @@ def test_oracle_matches_reference_snapshots(case, tmp_path):
             assert ora.scalar(k) == sc_ref[k], (case, target, k)
 
 
-def test_results_files_match_reference_program(tmp_path):
-    """Step the oracle through the plane case and write every output with the
+@pytest.mark.parametrize("case", ["plane_walls", "inflow"])
+def test_results_files_match_reference_program(case, tmp_path):
+    """Step the oracle through a case and write every output with the
     product's host writer; compare with the reference program's files."""
     from fluxos_cpp_b200 import write_results_host
-    sc, z, meta, _ = G.materialise("plane_walls", str(tmp_path))
+    sc, z, meta, _ = G.materialise(case, str(tmp_path))
     ora = P.OracleRun(str(tmp_path), sc, 0)
     files = meta["results"]
     out = tmp_path / "out"
