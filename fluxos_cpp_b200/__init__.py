@@ -58,7 +58,7 @@ class FxParams(C.Structure):
                 ("print_step", C.c_double), ("print_next", C.c_double), ("tim", C.c_double),
                 ("h_min_print", C.c_double), ("ade", C.c_int), ("volrat_mode", C.c_int),
                 ("d_coef", C.c_double * MAX_CHEM), ("steps_in_flight", C.c_int),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("wintra", C.c_int), ("soil_release_rate", C.c_double)]
 
 
 class FxStatus(C.Structure):
@@ -126,11 +126,11 @@ def lib() -> C.CDLL:
     L.fx_batch_stream.restype = vp
     L.fx_initiate.argtypes = [vp, dp]
     L.fx_load_modset.argtypes = [cp, C.POINTER(FxGrid), C.POINTER(FxParams), dp, dp, dp, dp, dp, dp,
-                                 dp, fp, fp, fp, C.POINTER(ip)]
+                                 dp, dp, fp, fp, fp, C.POINTER(ip)]
     L.fx_open_modset.argtypes = [cp, C.POINTER(vp)]
     L.fx_write_results.argtypes = [vp, cp]
     L.fx_write_results_host.argtypes = [cp, ip, ip, ip, C.c_double, C.c_double, C.c_double, dp, dp, dp,
-                                        dp, dp, dp, dp, dp, dp]
+                                        dp, dp, dp, dp, dp, dp, dp]
     L.fx_run.argtypes = [cp]
     _lib = L
     return L
@@ -158,17 +158,17 @@ def load_modset(path: str) -> dict:
     nul = C.POINTER(C.c_double)()
     nulf = C.POINTER(C.c_float)()
     _check(L.fx_load_modset(path.encode(), C.byref(g), C.byref(p), nul, nul, nul, nul, nul, nul, nul,
-                            nulf, nulf, nulf, None))
+                            nul, nulf, nulf, nulf, None))
     shape = (g.ncols + 2, g.nrows + 2)
-    out = {k: np.zeros(shape) for k in ("zb", "z", "h", "qx", "qy", "twet", "conc")}
+    out = {k: np.zeros(shape) for k in ("zb", "z", "h", "qx", "qy", "twet", "conc", "soil_mass")}
     out["ldry"] = np.zeros(shape, dtype=np.float32)
     out["wall"] = np.zeros(shape, dtype=np.float32)
     out["meteo"] = np.zeros((3, METEO_ROWS), dtype=np.float32)
     hm = C.c_int(0)
     _check(L.fx_load_modset(path.encode(), C.byref(g), C.byref(p), _dptr(out["zb"]), _dptr(out["z"]),
                             _dptr(out["h"]), _dptr(out["qx"]), _dptr(out["qy"]), _dptr(out["twet"]),
-                            _dptr(out["conc"]), _fptr(out["ldry"]), _fptr(out["wall"]),
-                            _fptr(out["meteo"]), C.byref(hm)))
+                            _dptr(out["conc"]), _dptr(out["soil_mass"]), _fptr(out["ldry"]),
+                            _fptr(out["wall"]), _fptr(out["meteo"]), C.byref(hm)))
     out["grid"] = {k: getattr(g, k) for k, _ in g._fields_}
     out["params"] = {k: getattr(p, k) for k, _ in p._fields_ if k != "d_coef"}
     out["params"]["d_coef"] = list(p.d_coef)
@@ -178,12 +178,15 @@ def load_modset(path: str) -> dict:
 
 def write_results_host(path: str, nrows: int, ncols: int, dxy: int, xll: float, yll: float,
                        h_min_print: float, grids: dict) -> None:
-    """write_results (write_results.cpp:30-101) on host grids."""
+    """write_results (write_results.cpp:30-101) on host grids; without a
+    "soil_mass" grid that column is 0."""
     a = {k: np.ascontiguousarray(grids[k], dtype=np.float64) for k in
          ("z", "zb", "h", "qx", "qy", "conc", "fe_1", "fn_1", "twet")}
+    soil_arr = np.ascontiguousarray(grids["soil_mass"], dtype=np.float64) if "soil_mass" in grids else None
+    soil = _dptr(soil_arr) if soil_arr is not None else C.POINTER(C.c_double)()
     _check(lib().fx_write_results_host(path.encode(), nrows, ncols, dxy, xll, yll, h_min_print,
                                        _dptr(a["z"]), _dptr(a["zb"]), _dptr(a["h"]), _dptr(a["qx"]),
-                                       _dptr(a["qy"]), _dptr(a["conc"]), _dptr(a["fe_1"]),
+                                       _dptr(a["qy"]), _dptr(a["conc"]), soil, _dptr(a["fe_1"]),
                                        _dptr(a["fn_1"]), _dptr(a["twet"])))
 
 
@@ -212,7 +215,7 @@ class Domain:
                  ntim: float = 0.0, print_step: float = 600.0, print_next: Optional[float] = None,
                  tim: float = 0.0, h_min_print: float = 0.0, ade: bool = True, volrat_mode: int = 0,
                  d_coef: Sequence[float] = (0.01,), steps_in_flight: int = 0, precision: str = "fp64",
-                 _handle=None):
+                 wintra: bool = False, soil_release_rate: float = 0.0, _handle=None):
         self.L = lib()
         self.nrows, self.ncols, self.dxy, self.nchem = nrows, ncols, dxy, nchem
         self.xll, self.yll, self.h_min_print = xll, yll, h_min_print
@@ -237,6 +240,8 @@ class Domain:
             p.d_coef[k] = float(d_coef[k] if k < len(d_coef) else d_coef[-1])
         p.steps_in_flight = int(steps_in_flight)
         p.precision = 1 if precision == "fp32" else 0
+        p.wintra = 1 if wintra else 0
+        p.soil_release_rate = float(soil_release_rate)
         h = C.c_void_p()
         _check(self.L.fx_create(C.byref(g), C.byref(p), C.byref(h)))
         self.h = h

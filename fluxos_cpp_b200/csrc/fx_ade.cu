@@ -95,6 +95,7 @@ struct Fields<double> {
   static __device__ __forceinline__ const double* fn1(const fx_dev& d) { return d.fn1; }
   static __device__ __forceinline__ const double* mm(const fx_dev& d) { return d.melt_mult; }
   static __device__ __forceinline__ double* conc(const fx_dev& d) { return d.conc; }
+  static __device__ __forceinline__ double* soil(const fx_dev& d) { return d.soil; }
 };
 template <>
 struct Fields<float> {
@@ -105,6 +106,7 @@ struct Fields<float> {
   static __device__ __forceinline__ const float* fn1(const fx_dev& d) { return d.fn1_f; }
   static __device__ __forceinline__ const float* mm(const fx_dev& d) { return d.melt_mult_f; }
   static __device__ __forceinline__ float* conc(const fx_dev& d) { return d.conc_f; }
+  static __device__ __forceinline__ float* soil(const fx_dev& d) { return d.soil_f; }
 };
 
 // Division and square root: IEEE-rounded in FP64 (bit parity with the
@@ -144,6 +146,7 @@ struct StepIn {
   double inflowi, iconc, inflow_hm;
   bool sweep;           // the sweep runs (hpall != 0 and it > 1)
   bool dilute;          // add_meteo's dilution runs
+  bool wintra;          // the soil release follows the sweep (hpall != 0)
 };
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
@@ -364,6 +367,28 @@ __device__ __forceinline__ void ade_cell(const fx_dev& d, T D, T dt, bool last_r
   qfn_out = qfn;
 }
 
+// wintrasolver_calc (WINTRAsolver_calc.cpp:39-57) at one cell after the
+// step's sweep, for solute k with concentration c: a wet cell whose bed is
+// not NODATA_VALUE releases soil * rate / 3600 * dt of its soil mass into
+// the concentration, c + deltam / (h * arbase). The reference calls it once
+// per solute on one soil grid (main.cpp:400-404); this solute's copy of the
+// soil mass replays every solute's release and keeps its own term. The soil
+// mass is read through L2 (other SMs wrote it in earlier steps).
+template <class T>
+__device__ __forceinline__ T soil_release(const fx_dev& d, const StepIn& S, int k, long long gi, T h, T c) {
+  if (!((double)h > d.hdry) || (d.flags[S.cur + gi] & FX_F_NODATA)) return c;
+  T* p = Fields<T>::soil(d) + (long long)k * d.plane + gi;
+  T soil = __ldcg(p);
+  T mine = T(0);
+  for (int j = 0; j < d.nchem; ++j) {
+    const T dm = tdiv(soil * (T)d.soil_rate, T(3600)) * (T)S.dt;
+    soil = soil - dm;
+    if (j == k) mine = dm;
+  }
+  *p = soil;
+  return c + tdiv(mine, h * (T)d.arbase);
+}
+
 // The three progress counters a unit depends on: the west strip of its step
 // and, on the previous step of the batch, its own strip and the next one.
 // The last values seen are kept, so a requirement the producer has already
@@ -436,6 +461,7 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
     S.dt = rec.dtfl;
     S.sweep = rec.active && rec.it > 1;  // :45,74-77
     S.dilute = d.has_meteo != 0;
+    S.wintra = d.wintra && rec.active;  // main.cpp:385-405
     S.inflow_gi = d.has_inflow ? d.inflow_gi : -1;
     S.inflowi = rec.inflowi;
     S.iconc = rec.iconc;
@@ -582,7 +608,9 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
                    EE_b, o_c, n1.b, NN_b, W_pfe, o_qfn, E_ld, W_ld, EE_ld, n1.ld, o_ld, NN_ld, cmax,
                    cmin, out_c, pfe, qfn);
         }
-        A[gi] = out_c;
+        // the sweep's neighbours and the next strip read the value before the
+        // soil release, which follows the whole sweep in the reference
+        A[gi] = S.wintra ? soil_release<T>(d, S, k, gi, cur.h, out_c) : out_c;
         if (lane == ROWS - 1 && bnd_out) {
           double* p = bnd_out + (long long)iy * 3;
           p[0] = (double)out_c;

@@ -5,6 +5,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -46,6 +47,7 @@ struct FieldRef {
   bool f32 = false;   // float (FP32 state) instead of double
   bool slot = false;  // one plane per slot
   bool pair = false;  // two planes, the current one is fx_pp(steps)
+  int copies = 1;     // identical planes (the soil mass: one per solute)
 };
 
 static FieldRef field_ref(fx_ctx* c, const char* name) {
@@ -77,12 +79,31 @@ static FieldRef field_ref(fx_ctx* c, const char* name) {
     if (k >= 0 && k < d.nchem)
       pick(d.conc ? d.conc + (long long)k * d.plane : nullptr,
            d.conc_f ? d.conc_f + (long long)k * d.plane : nullptr, false);
+  } else if (!strcmp(name, "soil_mass")) {
+    pick(d.soil, d.soil_f, false);
+    r.copies = d.nchem;
   }
   return r;
 }
 
+// "soil_mass" is allocated with the WINTRA module or by its first upload;
+// until then it reads as zeros.
 static bool known_field(fx_ctx* c, const char* name) {
-  return !strcmp(name, "z") || field_ref(c, name).ptr != nullptr;
+  return !strcmp(name, "z") || !strcmp(name, "soil_mass") || field_ref(c, name).ptr != nullptr;
+}
+
+static int dev_alloc(fx_ctx* c, void** p, size_t bytes);
+
+static int alloc_soil(fx_ctx* c) {
+  fx_dev& d = c->d;
+  if (d.soil || d.soil_f) return FX_OK;
+  const size_t bytes = (size_t)d.plane * d.nchem * (d.prec32 ? sizeof(float) : sizeof(double));
+  int rc = d.prec32 ? dev_alloc(c, (void**)&d.soil_f, bytes) : dev_alloc(c, (void**)&d.soil, bytes);
+  if (rc) return rc;
+  c->graph_dirty = true;
+  c->dev_dirty = true;
+  c->dev_version++;
+  return FX_OK;
 }
 
 static int dev_alloc(fx_ctx* c, void** p, size_t bytes) {
@@ -262,6 +283,8 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
   d.cfl_dxy = (double)(cfl * (float)g->dxy);
   d.volrat_mode = p->volrat_mode;
   d.ade = p->ade;
+  d.wintra = (p->wintra && p->ade) ? 1 : 0;  // main.cpp:209-213
+  d.soil_rate = p->soil_release_rate;
   for (int k = 0; k < FX_MAX_CHEM; ++k) d.dcoef[k] = p->d_coef[k];
   {
     int k = p->steps_in_flight > 0 ? p->steps_in_flight : 8;
@@ -301,6 +324,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
       if ((rc = dev_alloc(c, (void**)f, pf * d.nslot)) != FX_OK) goto fail;
     if ((rc = dev_alloc(c, (void**)&d.conc_f, pf * g->nchem)) != FX_OK) goto fail;
   }
+  if (d.wintra && (rc = alloc_soil(c)) != FX_OK) goto fail;
   if ((rc = dev_alloc(c, (void**)&c->d_mass, sizeof(double) * (1 + FX_MAX_CHEM))) != FX_OK) goto fail;
   if ((rc = dev_alloc(c, (void**)&d.flags, (size_t)d.plane * d.nslot)) != FX_OK) goto fail;
   if ((rc = dev_alloc(c, (void**)&d.ctl, sizeof(fx_ctl))) != FX_OK) goto fail;
@@ -399,6 +423,7 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
     b += plane * (8 + 5 * 4 + 4 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids);
   else
     b += plane * (6 * 8 + 3 * 2 * 8 + 5 * 8 * nslot + 8LL * g->nchem + 8LL * extension_grids);
+  if (p->wintra && p->ade) b += plane * g->nchem * (p->precision == 1 ? 4 : 8);  // soil mass
   b += plane * nslot;                                   // flags
   b += (long long)sizeof(fx_ctl) + 3 * FX_METEO_ROWS * 4 + (long long)sizeof(fx_dev);
   b += 8LL * nslot * g->nchem * strips * (g->ncols + 2) * 3 + 8LL * nslot * g->nchem * strips;
@@ -477,13 +502,14 @@ int fx_upload(fx_ctx* c, const char* field, const double* host) {
     }
     if ((rc = put_grid(c, c->d.zb, false, 1, host))) return rc;
   } else {
+    if (!strcmp(field, "soil_mass") && (rc = alloc_soil(c))) return rc;
     const FieldRef f = field_ref(c, field);
     // Every plane of a slot or pair field holds the uploaded grid: the steps
     // overwrite the interior cells only, and the ghost ring they read stays
     // as uploaded. The host grid crosses PCIe once, into the current plane;
     // the other planes are device-to-device copies of it.
     const size_t esz = f.f32 ? sizeof(float) : sizeof(double);
-    const int planes = f.slot ? c->d.nslot : (f.pair ? 2 : 1);
+    const int planes = f.slot ? c->d.nslot : (f.pair ? 2 : f.copies);
     long long cur = 0;
     if (planes > 1) {
       if ((rc = read_ctl(c))) return rc;
@@ -507,6 +533,10 @@ int fx_download(fx_ctx* c, const char* field, double* host) {
   if (!known_field(c, field)) return fx_fail(c, FX_ERR_ARG, "fx_download: unknown field '%s'", field);
   if (c->d.prec32 && !strcmp(field, "z")) return get_z32(c, host);
   const FieldRef f = field_ref(c, field);
+  if (!f.ptr) {  // soil_mass never set
+    std::fill(host, host + ((size_t)c->d.nr + 2) * ((size_t)c->d.nc + 2), 0.0);
+    return FX_OK;
+  }
   const size_t esz = f.f32 ? sizeof(float) : sizeof(double);
   const char* src = (const char*)f.ptr;
   if (f.slot || f.pair) {

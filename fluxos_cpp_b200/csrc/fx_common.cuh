@@ -110,7 +110,7 @@ struct fx_dev {
   // (eta, eta_lo, qx_f, qy_f) hold two planes: the state after step n is in
   // plane n & 1 (fx_pp).
   int nslot;
-  int pad3_;
+  int wintra;         // WINTRA soil release after each step's ADE sweep (needs ade)
   double *z, *zb, *h, *qx, *qy, *twet, *h0;
   double* hpm;        // per slot: the depth before the step's melt, max(z - zb, 0) (common.cpp:216)
   double *fe1, *fe2, *fe3, *fn1, *fn2, *fn3;
@@ -153,6 +153,14 @@ struct fx_dev {
   double* ade_bnd;                 // per slot, solute, strip: (ncols+2) x 3
   unsigned long long* ade_prog;    // per slot, solute, strip: step<<32 | warp steps done
   long long plane;                 // elements per field = ld * (nc + 2)
+  // WINTRA (WINTRAsolver_calc.cpp:26-58): the soil mass, one copy per solute
+  // in the state's precision. The reference releases into each solute in
+  // turn from one soil grid; each solute's sweep replays that whole
+  // sequence on its own copy, so the copies stay identical and no solute's
+  // sweep waits on another's.
+  double soil_rate;   // SOIL_RELEASE_RATE [1/hour]
+  double* soil;       // nchem planes (FP64 state)
+  float* soil_f;      // nchem planes (FP32 state)
 };
 
 // Work tables of a batch of domains (one domain is a batch of one).

@@ -223,6 +223,8 @@ struct Modset {
   unsigned long print_step = 0, h_min_print = 0;
   unsigned long inflow_x = 0, inflow_y = 0;  // DISCHARGE_LOCATION (GlobVar.h:100)
   double ks = 0.0, d_coef = 0.0;
+  bool wintra = false;                           // EXTERNAL_MODULES.WINTRA.STATUS
+  double soil_release_rate = 0.0, soil_conc_bckgrd = 0.0;  // GlobVar.h:95
 };
 
 // Numbers stored in unsigned long fields (GlobVar.h:102) truncate toward 0.
@@ -280,6 +282,11 @@ int read_modset(const std::string& path, Modset& m, std::string& err) {
   const JVal* ade = mods ? mods->get("ADE_TRANSPORT") : nullptr;
   m.ade = ade && as_bool(ade->get("STATUS"));
   if (m.ade) m.d_coef = as_double(ade->get("D_COEF"));
+  // read_functions.cpp:46-47,65
+  m.soil_release_rate = as_double(root.get("SOIL_RELEASE_RATE"));
+  m.soil_conc_bckgrd = as_double(root.get("SOIL_CONC_BACKGROUND"));
+  const JVal* wintra = mods ? mods->get("WINTRA") : nullptr;
+  m.wintra = wintra && as_bool(wintra->get("STATUS"));
   if ((v = root.get("METEO_FILE")) && v->kind == JVal::STR) {
     m.meteo_file = v->s;
     m.has_meteo = !m.meteo_file.empty();
@@ -444,7 +451,7 @@ int inflow_cell(const Modset& m, double xll, double yll, int dxy, int nrows, int
 // bed averaging, zero initial state and ghost ring (initiate.cpp:43-107,
 // 159-228). Outputs are full GlobVar grids.
 struct InitState {
-  std::vector<double> zb, z, h, qx, qy, ks, twet, conc0;
+  std::vector<double> zb, z, h, qx, qy, ks, twet, conc0, soil;
   std::vector<float> ldry, wall;
 };
 
@@ -460,6 +467,7 @@ void initiate_bed(int NR, int NC, double nodata, double ks_input, bool ade, cons
   s.ks.assign(n, 0.0);
   s.twet.assign(n, 0.0);
   s.conc0.assign(n, 0.0);
+  s.soil.assign(n, 0.0);
   s.ldry.assign(n, 0.0f);
   s.wall.assign(n, 0.0f);
   for (int icol = 1; icol <= NC; icol++) {
@@ -636,8 +644,8 @@ int fx_initiate(fx_ctx* c, const double* zb_raw) {
 // touches the GPU. Call once with all buffers NULL to learn the sizes (g, p),
 // then again with buffers of (nrows+2)*(ncols+2) elements (table: 3*2000).
 int fx_load_modset(const char* modset_path, fx_grid* g_out, fx_params* p_out, double* zb, double* z,
-                   double* h, double* qx, double* qy, double* twet, double* conc, float* ldry,
-                   float* wall, float* table_2000x3, int* has_meteo) {
+                   double* h, double* qx, double* qy, double* twet, double* conc, double* soil_mass,
+                   float* ldry, float* wall, float* table_2000x3, int* has_meteo) {
   if (!modset_path || !g_out || !p_out) return fx_fail(nullptr, FX_ERR_ARG, "fx_load_modset: null argument");
   Modset m;
   std::string err;
@@ -687,6 +695,8 @@ int fx_load_modset(const char* modset_path, fx_grid* g_out, fx_params* p_out, do
   p.ade = m.ade ? 1 : 0;
   p.volrat_mode = 0;
   p.d_coef[0] = m.d_coef;
+  p.wintra = (m.wintra && m.ade) ? 1 : 0;  // main.cpp:209-213
+  p.soil_release_rate = m.soil_release_rate;
   long long timstart = 0;
   if (m.restart) timstart = last_results_time(m.output_folder);
   p.tim = 0.0;  // GlobVar::tim is never assigned before the loop (main.cpp:271)
@@ -706,6 +716,13 @@ int fx_load_modset(const char* modset_path, fx_grid* g_out, fx_params* p_out, do
     auto rows = read_csv_numbers(fn, &ok);
     if (ok) {
       const size_t mr = (size_t)g.nrows + 2;
+      // initiate.cpp:93-107: the background soil mass where the bed is not
+      // 99999, before the file's rows
+      for (int icol = 1; icol <= g.ncols; icol++)
+        for (int irow = 1; irow <= g.nrows; irow++) {
+          const size_t i = (size_t)icol * mr + (size_t)irow;
+          if (std::fabs(s.zb[i]) != 99999) s.soil[i] = m.soil_conc_bckgrd;
+        }
       for (size_t a = 1; a < rows.size(); ++a) {
         const auto& r = rows[a];
         if (r.size() < 16) continue;
@@ -717,6 +734,7 @@ int fx_load_modset(const char* modset_path, fx_grid* g_out, fx_params* p_out, do
         s.qx[i] = r[8];
         s.qy[i] = r[9];
         s.conc0[i] = m.ade ? std::fmax(r[11], 0.0) : -1.0;
+        s.soil[i] = r[12];
         s.twet[i] = r[15];
         s.ldry[i] = 0.0f;
       }
@@ -731,6 +749,7 @@ int fx_load_modset(const char* modset_path, fx_grid* g_out, fx_params* p_out, do
   if (qy) std::copy(s.qy.begin(), s.qy.end(), qy);
   if (twet) std::copy(s.twet.begin(), s.twet.end(), twet);
   if (conc) std::copy(s.conc0.begin(), s.conc0.end(), conc);
+  if (soil_mass) std::copy(s.soil.begin(), s.soil.end(), soil_mass);
   if (ldry) std::copy(s.ldry.begin(), s.ldry.end(), ldry);
   if (wall) std::copy(s.wall.begin(), s.wall.end(), wall);
   if (table_2000x3) std::copy(tab.begin(), tab.end(), table_2000x3);
@@ -744,14 +763,14 @@ int fx_open_modset(const char* modset_path, fx_ctx** out) {
   fx_grid g{};
   fx_params p{};
   int rc = fx_load_modset(modset_path, &g, &p, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-                          nullptr, nullptr, nullptr, nullptr, nullptr);
+                          nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
   if (rc) return rc;
   const size_t n = ((size_t)g.nrows + 2) * ((size_t)g.ncols + 2);
-  std::vector<double> zb(n), z(n), h(n), qx(n), qy(n), tw(n), cc(n);
+  std::vector<double> zb(n), z(n), h(n), qx(n), qy(n), tw(n), cc(n), soil(n);
   std::vector<float> ldry(n), wall(n), tab(3 * FX_METEO_ROWS);
   int has_meteo = 0;
   rc = fx_load_modset(modset_path, &g, &p, zb.data(), z.data(), h.data(), qx.data(), qy.data(), tw.data(),
-                      cc.data(), ldry.data(), wall.data(), tab.data(), &has_meteo);
+                      cc.data(), soil.data(), ldry.data(), wall.data(), tab.data(), &has_meteo);
   if (rc) return rc;
   Modset m;
   std::string err;
@@ -764,7 +783,9 @@ int fx_open_modset(const char* modset_path, fx_ctx** out) {
       (rc = fx_upload(c, "h", h.data())) || (rc = fx_upload(c, "qx", qx.data())) ||
       (rc = fx_upload(c, "qy", qy.data())) || (rc = fx_upload(c, "twet", tw.data())) ||
       (rc = fx_upload(c, "conc", cc.data())) || (rc = fx_upload_flags(c, ldry.data(), wall.data())) ||
-      (rc = fx_set_forcing(c, tab.data(), has_meteo))) {
+      (rc = fx_set_forcing(c, tab.data(), has_meteo)) ||
+      ((p.wintra || std::any_of(soil.begin(), soil.end(), [](double v) { return v != 0.0; })) &&
+       (rc = fx_upload(c, "soil_mass", soil.data())))) {
     std::string e = c->err;
     fx_destroy(c);
     return fx_fail(nullptr, rc, "%s", e.c_str());
@@ -795,8 +816,9 @@ int fx_open_modset(const char* modset_path, fx_ctx** out) {
 
 int fx_write_results_host(const char* path, int nrows, int ncols, int dxy, double xll, double yll,
                           double h_min_print, const double* z, const double* zb, const double* h,
-                          const double* qx, const double* qy, const double* conc, const double* fe1,
-                          const double* fn1, const double* twet) {
+                          const double* qx, const double* qy, const double* conc,
+                          const double* soil_mass, const double* fe1, const double* fn1,
+                          const double* twet) {
   if (!path || !z || !zb || !h || !qx || !qy || !conc || !fe1 || !fn1 || !twet)
     return fx_fail(nullptr, FX_ERR_ARG, "fx_write_results_host: null argument");
   FILE* fp = fopen(path, "w");
@@ -816,7 +838,8 @@ int fx_write_results_host(const char* path, int nrows, int ncols, int dxy, doubl
       if (zb[i] != 0.0 && h[i] > h_min_print) {  // :280
         const double v[16] = {(double)irow, (double)icol, (double)((unsigned long)icol * (unsigned long)dxy) + xll,
                               (double)((unsigned long)irow * (unsigned long)dxy) + yll, z[i], z[i] - zb[i], 0.0,
-                              0.0, qx[i] * dx, qy[i] * dx, 0.0, conc[i], 0.0, fe1[i], fn1[i], twet[i]};
+                              0.0, qx[i] * dx, qy[i] * dx, 0.0, conc[i], soil_mass ? soil_mass[i] : 0.0,
+                              fe1[i], fn1[i], twet[i]};
         line.clear();
         for (int k = 0; k < 16; ++k) {
           line += fmt17(v[k]);
@@ -844,16 +867,16 @@ int fx_write_results(fx_ctx* c, const char* path) {
   if (path) fn = path;
   else fn = c->output_folder + "/" + std::to_string((long long)std::llround(st.print_next)) + ".txt";
   const size_t n = ((size_t)c->g.nrows + 2) * ((size_t)c->g.ncols + 2);
-  std::vector<double> z(n), zb(n), h(n), qx(n), qy(n), cc(n), fe(n), fnn(n), tw(n);
+  std::vector<double> z(n), zb(n), h(n), qx(n), qy(n), cc(n), sm(n), fe(n), fnn(n), tw(n);
   if ((rc = fx_download(c, "z", z.data())) || (rc = fx_download(c, "zb", zb.data())) ||
       (rc = fx_download(c, "h", h.data())) || (rc = fx_download(c, "qx", qx.data())) ||
       (rc = fx_download(c, "qy", qy.data())) || (rc = fx_download(c, "conc", cc.data())) ||
-      (rc = fx_download(c, "fe_1", fe.data())) || (rc = fx_download(c, "fn_1", fnn.data())) ||
-      (rc = fx_download(c, "twet", tw.data())))
+      (rc = fx_download(c, "soil_mass", sm.data())) || (rc = fx_download(c, "fe_1", fe.data())) ||
+      (rc = fx_download(c, "fn_1", fnn.data())) || (rc = fx_download(c, "twet", tw.data())))
     return rc;
   rc = fx_write_results_host(fn.c_str(), c->g.nrows, c->g.ncols, c->g.dxy, c->g.xll, c->g.yll,
                              c->h_min_print, z.data(), zb.data(), h.data(), qx.data(), qy.data(), cc.data(),
-                             fe.data(), fnn.data(), tw.data());
+                             sm.data(), fe.data(), fnn.data(), tw.data());
   if (rc) c->err = fx_last_error(nullptr);
   return rc;
 }

@@ -66,6 +66,12 @@ class Scenario:
     # coordinates, integers as the reference stores them (GlobVar.h:100).
     inflow: Optional[Sequence[Tuple[float, float, float]]] = None
     inflow_xy: Optional[Tuple[int, int]] = None
+    # WINTRA soil release (EXTERNAL_MODULES.WINTRA, SOIL_RELEASE_RATE [1/hour])
+    # and the soil mass per cell it releases (interior array; the reference
+    # only fills it from a restart file, initiate.cpp:93-152).
+    wintra: bool = False
+    soil_release_rate: float = 0.0
+    init_soil: Optional[np.ndarray] = None
     # Optional wet start (interior arrays, same shape as dem).
     init_h: Optional[np.ndarray] = None
     init_qx: Optional[np.ndarray] = None
@@ -108,12 +114,12 @@ class Scenario:
                 "H_MIN_TO_PRINT": self.h_min_print,
             },
             "ROUGNESS_HEIGHT": self.ks,
-            "SOIL_RELEASE_RATE": 0.0,
+            "SOIL_RELEASE_RATE": float(self.soil_release_rate),
             "SOIL_CONC_BACKGROUND": 0.0,
             "EXTERNAL_MODULES": {
                 "ADE_TRANSPORT": {"STATUS": bool(self.ade), "D_COEF": self.d_coef},
                 "OPENWQ": {"STATUS": False, "MASTERFILE_DIR": ""},
-                "WINTRA": {"STATUS": False, "SWE_STD": 0.0, "SWE_MAX": 0.0},
+                "WINTRA": {"STATUS": bool(self.wintra), "SWE_STD": 0.0, "SWE_MAX": 0.0},
             },
         }
         if self.inflow is not None:
@@ -339,7 +345,8 @@ def make_domain(sc: Scenario, *, precision: str = "fp64", steps_in_flight: int =
     d = fx.Domain(sc.nrows, sc.ncols, sc.dxy, nchem=sc.nchem, nodata=float(sc.nodata), hdry=sc.ks,
                   ntim=sc.horizon, print_step=sc.print_step, print_next=sc.print_step, ade=sc.ade,
                   d_coef=list(sc.d_coefs) if sc.d_coefs else [sc.d_coef],
-                  steps_in_flight=steps_in_flight, precision=precision)
+                  steps_in_flight=steps_in_flight, precision=precision, wintra=sc.wintra,
+                  soil_release_rate=sc.soil_release_rate)
     d.initiate(full_grid(sc, sc.dem.astype(np.float64)))
     d.set_forcing(forcing_table(sc))
     if sc.inflow is not None:
@@ -362,6 +369,8 @@ def make_domain(sc: Scenario, *, precision: str = "fp64", steps_in_flight: int =
         fl = d.download_flags()
         ld = full_grid(sc, np.where(sc.init_h > sc.ks, 0.0, 1.0))
         d.upload_flags(ld, fl["wall"])
+    if sc.init_soil is not None:
+        d.upload("soil_mass", full_grid(sc, sc.init_soil))
     d.prepare()
     return d
 

@@ -71,6 +71,11 @@ typedef struct fx_params {
                           FP32; the clock, the wet/dry threshold tests and the
                           water budget stay FP64. Not bit-compatible with the
                           reference: see tests/test_gpu_fp32.py for its error. */
+  int wintra;          /* EXTERNAL_MODULES.WINTRA.STATUS: the soil release of
+                          wintrasolver_calc (WINTRAsolver_calc.cpp:26-58) after
+                          each step's ADE sweep; off unless ade is on
+                          (main.cpp:209-213) */
+  double soil_release_rate; /* SOIL_RELEASE_RATE [1/hour] */
 } fx_params;
 
 /* Clock and status read back from the device. */
@@ -103,7 +108,9 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
 
 /* --- state ---------------------------------------------------------------
  * Field names: "z" "zb" "h" "qx" "qy" "twet" "h0" "fe_1" "fe_2" "fe_3"
- * "fn_1" "fn_2" "fn_3" "conc" (solute 0) "conc1".."conc7".
+ * "fn_1" "fn_2" "fn_3" "conc" (solute 0) "conc1".."conc7" "soil_mass" (the
+ * soil mass WINTRA releases [g]; 0 until uploaded, as the reference's
+ * initiation leaves it without a restart file).
  * Uploads take the full (nrows+2) x (ncols+2) grid; fx_upload_flags takes the
  * float flag grids ldry and innerNeumannBCWeir (wall) of GlobVar. After the
  * state is complete call fx_prepare once (it runs the first Courant scan). */
@@ -228,8 +235,8 @@ int fx_initiate(fx_ctx* ctx, const double* zb_raw);
  * sizes), then with arrays of (nrows+2)*(ncols+2) elements and a 3*2000
  * forcing table. */
 int fx_load_modset(const char* modset_path, fx_grid* g, fx_params* p, double* zb, double* z,
-                   double* h, double* qx, double* qy, double* twet, double* conc, float* ldry,
-                   float* wall, float* table_2000x3, int* has_meteo);
+                   double* h, double* qx, double* qy, double* twet, double* conc, double* soil_mass,
+                   float* ldry, float* wall, float* table_2000x3, int* has_meteo);
 /* Start-up of main.cpp:87-262 from a modset file: reads the master file
  * (with comments), the ESRI ASCII DEM, the forcing CSV, applies initiation
  * (bed averaging, zero or restart initial state, ghost ring), uploads. */
@@ -237,11 +244,13 @@ int fx_open_modset(const char* modset_path, fx_ctx** out);
 /* write_results (write_results.cpp:30-101): Results/<t>.txt of the current
  * state; path NULL means <OUTPUT_FOLDER>/<print_next>.txt. */
 int fx_write_results(fx_ctx* ctx, const char* path);
-/* The writer itself on host grids (no GPU needed). */
+/* The writer itself on host grids (no GPU needed); soil_mass may be NULL
+ * (a column of zeros). */
 int fx_write_results_host(const char* path, int nrows, int ncols, int dxy, double xll, double yll,
                           double h_min_print, const double* z, const double* zb, const double* h,
-                          const double* qx, const double* qy, const double* conc, const double* fe_1,
-                          const double* fn_1, const double* twet);
+                          const double* qx, const double* qy, const double* conc,
+                          const double* soil_mass, const double* fe_1, const double* fn_1,
+                          const double* twet);
 /* The whole program: open, step, write every output, close. */
 int fx_run(const char* modset_path);
 

@@ -33,6 +33,8 @@ struct ox_state {
   double hpall;
   int ade, has_meteo, has_inflow, volrat_mode;
   unsigned long inflow_nrow, inflow_ncol;
+  int wintra;               /* EXTERNAL_MODULES.WINTRA.STATUS (main.cpp:209-213: off without ADE) */
+  double soil_release_rate; /* SOIL_RELEASE_RATE [1/hour] (GlobVar.h:95) */
   /* grids */
   double *z, *zb, *h, *ux, *uy, *qx, *qy, *qxf, *qyf, *us, *dh, *dqx, *dqy, *ks;
   double *fe_1, *fe_2, *fe_3, *fn_1, *fn_2, *fn_3, *twet, *h0, *soil_mass;
@@ -164,6 +166,8 @@ double ox_scalar(ox_state* s, const char* n) {
   if (!strcmp(n, "volrat_mode")) return s->volrat_mode;
   if (!strcmp(n, "inflow_nrow")) return (double)s->inflow_nrow;
   if (!strcmp(n, "inflow_ncol")) return (double)s->inflow_ncol;
+  if (!strcmp(n, "wintra")) return s->wintra;
+  if (!strcmp(n, "soil_release_rate")) return s->soil_release_rate;
   return NAN;
 }
 
@@ -190,6 +194,8 @@ void ox_set_scalar(ox_state* s, const char* n, double v) {
   else if (!strcmp(n, "volrat_mode")) s->volrat_mode = (int)v;
   else if (!strcmp(n, "inflow_nrow")) s->inflow_nrow = (unsigned long)v;
   else if (!strcmp(n, "inflow_ncol")) s->inflow_ncol = (unsigned long)v;
+  else if (!strcmp(n, "wintra")) s->wintra = (int)v;
+  else if (!strcmp(n, "soil_release_rate")) s->soil_release_rate = v;
 }
 
 void ox_set_manning(ox_state* s, const double* n_field) { s->manning = n_field; }
@@ -1098,6 +1104,27 @@ void ox_adesolver(ox_state* s, int it, int ichem) {
 
 /* One iteration of main.cpp:273-406 (printing excluded; WINTRA and OpenWQ
  * are outside this path). Returns 1 if a forcing table ran out. */
+/* wintrasolver_calc (WINTRAsolver_calc.cpp:26-58) for solute ichem: every
+ * wet cell whose bed is not NODATA_VALUE releases the first-order fraction
+ * soil_release_rate/3600*dtfl of its soil mass into its concentration. The
+ * reference also computes a tanh melt factor (:33-36) that nothing reads;
+ * it is not restated. */
+void ox_wintra(ox_state* s, int ichem) {
+  double* c = s->conc + (size_t)ichem * s->ncell;
+  for (int icol = 1; icol <= s->ncols; icol++) {
+    for (int irow = 1; irow <= s->nrows; irow++) {
+      const size_t i = IX(s, irow, icol);
+      const double hp = s->h[i];
+      const double zbp = s->zb[i];
+      if (hp > s->hdry && zbp != s->nodata) {
+        const double deltam = s->soil_mass[i] * s->soil_release_rate / 3600 * s->dtfl;
+        s->soil_mass[i] = s->soil_mass[i] - deltam;
+        c[i] = c[i] + deltam / (hp * (double)s->arbase);
+      }
+    }
+  }
+}
+
 int ox_step(ox_state* s) {
   int err = 0;
   ox_courant(s);
@@ -1110,6 +1137,8 @@ int ox_step(ox_state* s) {
     ox_manning(s);
     if (s->ade)
       for (int k = 0; k < s->nchem; ++k) ox_adesolver(s, (int)s->it, k);
+    if (s->ade && s->wintra)  /* main.cpp:399-404 */
+      for (int k = 0; k < s->nchem; ++k) ox_wintra(s, k);
   }
   return err;
 }

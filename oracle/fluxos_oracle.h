@@ -47,6 +47,7 @@ int ox_add_inflow(ox_state* s);                 /* common.cpp:277-390 */
 void ox_hydrodynamics(ox_state* s);             /* hydrodynamics_calc.cpp:27-157 */
 void ox_adesolver(ox_state* s, int it, int ichem); /* ADEsolver_calc.cpp:27-291 */
 void ox_manning(ox_state* s);                   /* extension, after the hydro update */
+void ox_wintra(ox_state* s, int ichem);         /* WINTRAsolver_calc.cpp:26-58 */
 int ox_step(ox_state* s);                       /* main.cpp:273-406 without printing */
 int ox_running(ox_state* s);                    /* main.cpp:271 loop condition */
 int ox_print_due(ox_state* s);                  /* main.cpp:444 */

@@ -179,6 +179,8 @@ class OracleRun(_Run):
         L.ox_set_scalar(s, b"print_step", float(sc.print_step))
         L.ox_set_scalar(s, b"ade", 1.0 if sc.ade else 0.0)
         L.ox_set_scalar(s, b"volrat_mode", float(volrat_mode))
+        L.ox_set_scalar(s, b"wintra", 1.0 if (sc.wintra and sc.ade) else 0.0)  # main.cpp:209-213
+        L.ox_set_scalar(s, b"soil_release_rate", float(sc.soil_release_rate))
         if sc.d_coefs:
             for k, d in enumerate(sc.d_coefs):
                 L.ox_set_scalar(s, f"D_coef{k}".encode(), float(d))

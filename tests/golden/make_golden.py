@@ -31,7 +31,7 @@ import pyoracle as P  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SNAP_GRIDS = ("z", "h", "qx", "qy", "conc", "fe_1", "fe_2", "fe_3", "fn_1", "fn_2", "fn_3",
-              "twet", "h0", "ldry", "ldry_prev", "zb", "wall", "ks")
+              "twet", "h0", "ldry", "ldry_prev", "zb", "wall", "ks", "soil_mass")
 
 
 def case_plane_walls() -> dict:
@@ -84,12 +84,27 @@ def case_inflow() -> dict:
     return dict(sc=sc, wet=None, steps=(1, 10, 200, 2000), mode=0, results=True)
 
 
+def case_wintra() -> dict:
+    """The WINTRA soil release (EXTERNAL_MODULES.WINTRA) on a wet patchwork
+    under melt, with a seeded soil mass per cell (what a restart file's
+    soil_mass column would hold)."""
+    sc = S.plane_scenario(24, 20, seed=4)
+    sc.horizon = 3000.0
+    sc.wintra = True
+    sc.soil_release_rate = 0.8
+    sc.dem[5, 2:6] = -9999.0
+    rng = np.random.default_rng(11)
+    soil = rng.uniform(0.0, 50.0, (24, 20)) * (rng.random((24, 20)) < 0.7)
+    return dict(sc=sc, wet=_patch(24, 20, 5), soil=soil, steps=(1, 10, 100, 400), mode=0, results=False)
+
+
 CASES = {
     "plane_walls": case_plane_walls,
     "patchwork_weir": lambda: case_patchwork(0),
     "patchwork_closed": lambda: case_patchwork(1),
     "dambreak": case_dambreak,
     "inflow": case_inflow,
+    "wintra": case_wintra,
 }
 
 
@@ -105,7 +120,8 @@ def build_case(name: str, spec: dict) -> None:
     meta = dict(name=name, nrows=sc.nrows, ncols=sc.ncols, dxy=sc.dxy, nodata=sc.nodata,
                 print_step=sc.print_step, ks=sc.ks, ade=sc.ade, d_coef=sc.d_coef,
                 h_min_print=sc.h_min_print, volrat_mode=mode, steps=list(spec["steps"]),
-                wet=spec["wet"] is not None)
+                wet=spec["wet"] is not None, wintra=bool(sc.wintra),
+                soil_release_rate=float(sc.soil_release_rate))
     if sc.inflow is not None:
         with open(os.path.join(work, "inflow.csv")) as f:
             out["inflow_csv"] = np.array(f.read())
@@ -118,6 +134,9 @@ def build_case(name: str, spec: dict) -> None:
         for k in ("h", "qx", "qy"):
             out[f"wet_{k}"] = w[k]
         out["wet_conc0"] = w["conc"][0]
+    if spec.get("soil") is not None:
+        ref.interior("soil_mass")[...] = spec["soil"].T
+        out["soil0"] = spec["soil"]
     done = 0
     scal = {}
     for target in spec["steps"]:

@@ -7,7 +7,7 @@ import numpy as np
 from fluxos_cpp_b200 import scenarios as S
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ("plane_walls", "patchwork_weir", "patchwork_closed", "dambreak", "inflow")
+CASES = ("plane_walls", "patchwork_weir", "patchwork_closed", "dambreak", "inflow", "wintra")
 
 
 def load(name: str):
@@ -27,16 +27,18 @@ def materialise(name: str, folder: str):
     sc = S.Scenario(name=name, dem=np.zeros((meta["nrows"], meta["ncols"]), dtype=np.float32),
                     dxy=meta["dxy"], nodata=meta["nodata"], print_step=meta["print_step"],
                     ks=meta["ks"], ade=meta["ade"], d_coef=meta["d_coef"],
-                    h_min_print=meta["h_min_print"])
+                    h_min_print=meta["h_min_print"], wintra=meta.get("wintra", False),
+                    soil_release_rate=meta.get("soil_release_rate", 0.0))
     modset = {
         "DEM_FILE": os.path.join(folder, "dem.asc"), "SIM_DATETIME_START": "2020JAN01 00:00:00",
         "RESTART": False, "METEO_FILE": os.path.join(folder, "meteo.csv"),
         "OUTPUT": {"OUTPUT_FOLDER": os.path.join(folder, "Results"),
                    "PRINT_STEP": meta["print_step"], "H_MIN_TO_PRINT": meta["h_min_print"]},
-        "ROUGNESS_HEIGHT": meta["ks"], "SOIL_RELEASE_RATE": 0.0, "SOIL_CONC_BACKGROUND": 0.0,
+        "ROUGNESS_HEIGHT": meta["ks"], "SOIL_RELEASE_RATE": sc.soil_release_rate,
+        "SOIL_CONC_BACKGROUND": 0.0,
         "EXTERNAL_MODULES": {"ADE_TRANSPORT": {"STATUS": meta["ade"], "D_COEF": meta["d_coef"]},
                              "OPENWQ": {"STATUS": False, "MASTERFILE_DIR": ""},
-                             "WINTRA": {"STATUS": False, "SWE_STD": 0.0, "SWE_MAX": 0.0}},
+                             "WINTRA": {"STATUS": sc.wintra, "SWE_STD": 0.0, "SWE_MAX": 0.0}},
     }
     if "inflow_csv" in z.files:
         with open(os.path.join(folder, "inflow.csv"), "w") as f:
@@ -55,3 +57,12 @@ def materialise(name: str, folder: str):
 
 def wet_arrays(z):
     return dict(h=z["wet_h"], qx=z["wet_qx"], qy=z["wet_qy"], conc=[z["wet_conc0"]])
+
+
+def apply_start(run, z, meta) -> None:
+    """The case's wet start and seeded soil mass on an oracle run."""
+    if meta["wet"]:
+        w = wet_arrays(z)
+        run.apply_wet_start(w["h"], w["qx"], w["qy"], w["conc"])
+    if "soil0" in z.files:
+        run.interior("soil_mass")[...] = z["soil0"].T

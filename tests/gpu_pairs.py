@@ -15,13 +15,16 @@ def domain_from_oracle(ora, sc, volrat_mode=0, store_all=True, steps_in_flight=0
                   print_next=ora.scalar("print_next"), tim=ora.scalar("tim"), ade=sc.ade,
                   volrat_mode=volrat_mode,
                   d_coef=list(sc.d_coefs) if sc.d_coefs else [sc.d_coef],
-                  steps_in_flight=steps_in_flight)
+                  steps_in_flight=steps_in_flight, wintra=bool(ora.scalar("wintra")),
+                  soil_release_rate=ora.scalar("soil_release_rate"))
     for k in ("zb",) + STATE:
         d.upload(k, ora.grid(k))
     for k in range(nchem):
         nm = "conc" if k == 0 else f"conc{k}"
         d.upload(nm, ora.grid(nm))
     d.upload_flags(ora.grid("ldry"), ora.grid("wall"))
+    if ora.grid("soil_mass").any():
+        d.upload("soil_mass", ora.grid("soil_mass"))
     d.set_forcing(ora.fgrid("meteo"))
     if ora.scalar("has_inflow"):
         d.set_inflow(ora.fgrid("inflow"), int(ora.scalar("inflow_nrow")), int(ora.scalar("inflow_ncol")))
@@ -75,7 +78,7 @@ def compare(ora, d, sc, fields=STATE, rtol=1e-10):
     """Per-field max relative error (floored at 1e-6 of the field's scale)
     and the number of cells whose wet/dry flags differ."""
     out = {}
-    for k in list(fields) + [("conc" if i == 0 else f"conc{i}") for i in range(sc.nchem)]:
+    for k in list(fields) + [("conc" if i == 0 else f"conc{i}") for i in range(sc.nchem)] + ["soil_mass"]:
         a = ora.grid(k)[1:-1, 1:-1]
         b = d.download(k)[1:-1, 1:-1]
         scale = max(float(np.nanmax(np.abs(a))) if a.size else 0.0, 1e-300) * 1e-6

@@ -33,4 +33,4 @@ def test_errors_without_a_context_are_reported():
     assert b"nrows" in L.fx_last_error(None)
     assert not h.value
     assert L.fx_load_modset(b"/nonexistent/modset.json", ctypes.byref(g), ctypes.byref(p), None, None,
-                            None, None, None, None, None, None, None, None, None) == -3  # FX_ERR_IO
+                            None, None, None, None, None, None, None, None, None, None) == -3  # FX_ERR_IO

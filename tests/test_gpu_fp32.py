@@ -148,6 +148,28 @@ def test_fp32_point_inflow():
     assert abs(b32["melt_in"] - b64["melt_in"]) <= 1e-3 * b64["melt_in"]
 
 
+def test_fp32_wintra_soil_release():
+    """WINTRA in FP32: the soil mass and the solute mass it feeds follow the
+    FP64 path at equal times."""
+    sc = _fractal(192)
+    sc.wintra, sc.soil_release_rate = True, 1.5
+    sc.init_soil = np.random.default_rng(21).uniform(0.0, 80.0, (192, 192))
+    sc.print_step = 5
+    d64, d32 = S.make_domain(sc, precision="fp64"), S.make_domain(sc, precision="fp32")
+    s0 = d64.download("soil_mass").sum()
+    for t in (5.0, 20.0):
+        for d in (d64, d32):
+            _run_to(d, t)
+        s64, s32 = d64.download("soil_mass"), d32.download("soil_mass")
+        ls = float(np.abs(s32 - s64).sum() / np.abs(s64).sum())
+        e = A.state_errors(d32, d64, sc.ks)
+        print("wintra192", t, "soil L1 %.3e solute-mass L1 %.3e depth L1 %.3e"
+              % (ls, e["solute_mass_density"][0]["l1_rel"], e["depth"]["l1_rel"]))
+        assert ls <= 1e-5, (t, ls)
+        assert e["solute_mass_density"][0]["l1_rel"] <= 1e-3, (t, e)
+    assert d64.download("soil_mass").sum() < s0
+
+
 def test_fp32_state_stays_finite():
     """The large-domain workload's wet start (5 mm film plus ponded
     depressions) on steep fractal terrain: FP32 Ritter inflows whose surface
@@ -194,6 +216,8 @@ def test_fp32_batch_bit_identical_to_alone():
     scs = [_fractal(n) for n in (64, 150)]
     scs[1].inflow = ((0.0, 0.0, 0.0), (1e4, 0.1, 2.0))
     scs[1].inflow_xy = (2 * 70, 2 * 40)
+    scs[0].wintra, scs[0].soil_release_rate = True, 1.0
+    scs[0].init_soil = np.full((64, 64), 20.0)
     batched = [S.make_domain(sc, precision="fp32", steps_in_flight=4) for sc in scs]
     alone = [S.make_domain(sc, precision="fp32", steps_in_flight=4) for sc in scs]
     b = fx.Batch()
@@ -204,7 +228,7 @@ def test_fp32_batch_bit_identical_to_alone():
         d.step(57)
     for x, y in zip(batched, alone):
         assert x.status()["steps"] == y.status()["steps"] == 57
-        for k in ("z", "h", "qx", "qy", "conc", "fe_1", "fn_1"):
+        for k in ("z", "h", "qx", "qy", "conc", "fe_1", "fn_1", "soil_mass"):
             assert np.array_equal(x.download(k), y.download(k)), k
     with pytest.raises(fx.FluxosError):
         b.add(S.make_domain(scs[0], precision="fp64"))

@@ -22,9 +22,7 @@ pytestmark = pytest.mark.gpu
 def _pair_from_case(case, tmp_path, store_all=True):
     sc, z, meta, _ = G.materialise(case, str(tmp_path))
     ora = P.OracleRun(str(tmp_path), sc, meta["volrat_mode"])
-    if meta["wet"]:
-        w = G.wet_arrays(z)
-        ora.apply_wet_start(w["h"], w["qx"], w["qy"], w["conc"])
+    G.apply_start(ora, z, meta)
     d = GP.domain_from_oracle(ora, sc, meta["volrat_mode"], store_all)
     return sc, z, meta, ora, d
 
@@ -194,4 +192,31 @@ def test_point_inflow_parity(tma, in_flight, cell, tmp_path):
         res, bad = GP.compare(ora, d, sc)
         assert not bad, (n, bad)
     assert ora.scalar("tim") > 150.0  # every discharge row was used
+    d.close()
+
+
+@pytest.mark.parametrize("in_flight,nchem", [(8, 1), (31, 2), (1, 3)])
+def test_wintra_soil_release_parity(in_flight, nchem, tmp_path):
+    """The WINTRA soil release fused into the ADE sweep's store, with several
+    steps in flight and one or more solutes (each solute's sweep replays the
+    reference's per-solute sequence on its own copy of the soil mass)."""
+    nr, nc = 150, 130
+    sc = _random_scenario(nr, nc, 51)
+    sc.wintra, sc.soil_release_rate = True, 2.0
+    if nchem > 1:
+        sc.d_coefs = [0.01 * (k + 1) for k in range(nchem)]
+    sc.write(str(tmp_path))
+    ora = P.OracleRun(str(tmp_path), sc, 0)
+    rng = np.random.default_rng(8)
+    h = np.where(rng.random((nr, nc)) < 0.6, rng.uniform(0, 0.03, (nr, nc)), 0.0)
+    ora.apply_wet_start(h, None, None, [np.where(h > 0.01, 1.0 + k, 0.0) for k in range(nchem)])
+    ora.interior("soil_mass")[...] = (rng.uniform(0, 100.0, (nr, nc)) * (rng.random((nr, nc)) < 0.8)).T
+    d = GP.domain_from_oracle(ora, sc, 0, steps_in_flight=in_flight)
+    soil0 = ora.grid("soil_mass").sum()
+    for n in (1, 20, 150, 300):
+        GP.advance_oracle(ora, n)
+        GP.advance_domain(d, n)
+        res, bad = GP.compare(ora, d, sc)
+        assert not bad, (n, bad)
+    assert ora.grid("soil_mass").sum() < 0.999 * soil0  # the release happened
     d.close()

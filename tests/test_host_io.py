@@ -100,14 +100,16 @@ def test_restart_reads_newest_results_file(tmp_path):
     mp = sc.write(str(tmp_path))
     m = json.loads(open(mp).read().split("\n", 1)[1])
     m["RESTART"] = True
+    m["SOIL_CONC_BACKGROUND"] = 3.5
     open(mp, "w").write(json.dumps(m))
     res = os.path.join(str(tmp_path), "Results")
     os.makedirs(res)
     st0 = fx.load_modset(mp)  # no file yet: zero state, print_next = 0 + 600
     assert st0["params"]["print_next"] == 600.0
+    assert not st0["soil_mass"].any()  # initiate.cpp:177 without a file
     zb = st0["zb"]
     rows = ["h"] + [",".join(["3", "4", "0", "0", repr(float(zb[4, 3]) + 0.25), "0.25", "0", "0", "0.5", "-0.5",
-                              "0", "2.0", "0", "0", "0", "7.5"])]
+                              "0", "2.0", "4.25", "0", "0", "7.5"])]
     open(os.path.join(res, "1200.txt"), "w").write("\n".join(rows) + "\n")
     open(os.path.join(res, "600.txt"), "w").write("h\n")
     st = fx.load_modset(mp)
@@ -116,6 +118,39 @@ def test_restart_reads_newest_results_file(tmp_path):
     assert st["qx"][4, 3] == 0.5 and st["qy"][4, 3] == -0.5
     assert st["conc"][4, 3] == 2.0 and st["twet"][4, 3] == 7.5
     assert st["ldry"][4, 3] == 0.0 and st["ldry"][4, 4] == 1.0
+    # soil mass: the file's column 12, SOIL_CONC_BACKGROUND on the other
+    # interior cells (initiate.cpp:93-107,152), 0 on the ghost ring
+    soil = st["soil_mass"]
+    assert soil[4, 3] == 4.25 and soil[1, 1] == 3.5 and soil[0, 0] == 0.0
+    assert np.all(soil[1:-1, 1:-1][np.abs(zb[1:-1, 1:-1]) != 99999] > 0)
+
+
+def test_wintra_settings_are_read(tmp_path):
+    """SOIL_RELEASE_RATE and EXTERNAL_MODULES.WINTRA.STATUS (read_functions.cpp:46,65);
+    WINTRA is switched off without the ADE module (main.cpp:209-213)."""
+    sc = S.plane_scenario(6, 5)
+    sc.wintra, sc.soil_release_rate = True, 0.25
+    st = fx.load_modset(sc.write(str(tmp_path / "a")))
+    assert st["params"]["wintra"] == 1 and st["params"]["soil_release_rate"] == 0.25
+    sc.ade = False
+    st = fx.load_modset(sc.write(str(tmp_path / "b")))
+    assert st["params"]["wintra"] == 0
+
+
+def test_results_writer_soil_mass_column(tmp_path):
+    sc = S.plane_scenario(5, 4)
+    grids = {k: np.zeros((6, 7)) for k in ("z", "h", "qx", "qy", "conc", "fe_1", "fn_1", "twet")}
+    grids["zb"] = np.full((6, 7), 10.0)
+    grids["h"][2, 3] = 0.5
+    grids["z"] = grids["zb"] + grids["h"]
+    grids["soil_mass"] = np.zeros((6, 7))
+    grids["soil_mass"][2, 3] = 12.125
+    fn = str(tmp_path / "600.txt")
+    fx.write_results_host(fn, 5, 4, 2, 0.0, 0.0, 0.0, grids)
+    rows = open(fn).read().strip().split("\n")
+    assert len(rows) == 2
+    v = [float(x) for x in rows[1].split(",")]
+    assert (v[0], v[1], v[12]) == (3.0, 2.0, 12.125)
 
 
 def test_results_writer_empty_domain_writes_one_zero_row(tmp_path):

@@ -10,16 +10,14 @@ import golden_cases as G
 import pyoracle as P
 
 SNAP = ("z", "h", "qx", "qy", "conc", "fe_1", "fe_2", "fe_3", "fn_1", "fn_2", "fn_3", "twet", "h0",
-        "ldry", "ldry_prev", "zb", "wall", "ks")
+        "ldry", "ldry_prev", "zb", "wall", "ks", "soil_mass")
 
 
 @pytest.mark.parametrize("case", G.CASES)
 def test_oracle_matches_reference_snapshots(case, tmp_path):
     sc, z, meta, _ = G.materialise(case, str(tmp_path))
     ora = P.OracleRun(str(tmp_path), sc, meta["volrat_mode"])
-    if meta["wet"]:
-        w = G.wet_arrays(z)
-        ora.apply_wet_start(w["h"], w["qx"], w["qy"], w["conc"])
+    G.apply_start(ora, z, meta)
     done = 0
     for target in meta["steps"]:
         while done < target:
@@ -52,7 +50,8 @@ def test_results_files_match_reference_program(case, tmp_path):
         if ora.print_due():
             pn = int(round(ora.scalar("print_next")))
             fn = str(out / f"{pn}.txt")
-            grids = {k: ora.grid(k) for k in ("z", "zb", "h", "qx", "qy", "conc", "fe_1", "fn_1", "twet")}
+            grids = {k: ora.grid(k) for k in ("z", "zb", "h", "qx", "qy", "conc", "soil_mass", "fe_1", "fn_1",
+                                              "twet")}
             write_results_host(fn, sc.nrows, sc.ncols, sc.dxy, sc.xll, sc.yll, meta["h_min_print"], grids)
             written.append(f"{pn}.txt")
             ora.print_done()
