@@ -24,7 +24,14 @@ Also reported on the same line (skipped with --no-mix / --no-serve):
   batch (autotuned tiles), against the same scenarios as an FP64 batch and
   run one by one on the plain FP64 path;
 * serve: a bounded sample of the serving configuration's request stream
-  through the continuous-batching loop, with p50/p99 latency.
+  through the continuous-batching loop, with p50/p99 latency;
+* dambreak (--no-dambreak): the circular dam break (2048^2 cells of 1 m,
+  2 m of water within 300 m, flat bed, Manning n 0.02, two solutes, 600 s)
+  run to its horizon in FP64 and FP32: front position along 8 rays, depth
+  and discharge error of FP32 against FP64, both water balances;
+* results_writer (--no-writer): one Results file of the headline state
+  written from rows compacted on the device, asynchronously, and by the
+  host writer from downloaded grids (text into /dev/null).
 
 --impl reference times the FLUXOS reference sources compiled in oracle/_ref
 (OpenMP hydrodynamics, serial ADE) on the host cores instead.
@@ -201,6 +208,29 @@ def e2e_run(d, sc, steps: int, chunk: int):
     return t1 - t0, h2d, d2h
 
 
+def results_writer_timing(d, target: str = "/dev/null") -> dict:
+    """One Results file of the current state three ways, into `target`:
+    rows compacted on the device then formatted on host threads
+    (fx_write_results); the same started with fx_write_results_async, whose
+    return is all the stepping waits for; and the host writer on the ten
+    downloaded grids."""
+    import fluxos_cpp_b200 as fx
+    t0 = time.perf_counter()
+    d.write_results(target)
+    t1 = time.perf_counter()
+    d.write_results(target, wait=False)
+    t2 = time.perf_counter()
+    d.results_wait()
+    t3 = time.perf_counter()
+    g = {k: d.download(k) for k in ("z", "zb", "h", "qx", "qy", "conc", "soil_mass", "fe_1", "fn_1", "twet")}
+    fx.write_results_host(target, d.nrows, d.ncols, d.dxy, d.xll, d.yll, d.h_min_print, g)
+    t4 = time.perf_counter()
+    rows = int(((g["zb"][1:-1, 1:-1] != 0) & (g["h"][1:-1, 1:-1] > d.h_min_print)).sum())
+    return {"rows": rows, "device_compaction_s": t1 - t0, "async_start_s": t2 - t1,
+            "async_total_s": t3 - t1, "host_from_downloads_s": t4 - t3,
+            "note": "text into /dev/null; async_start_s is the stall the stepping sees"}
+
+
 class _stdout_to_stderr:
     """The reference's start-up prints progress to stdout (fd 1); keep the
     one JSON line of this program alone there."""
@@ -360,6 +390,58 @@ def run_mix(args, peak: float) -> dict:
                     "the batch stream); plain FP64 = each scenario alone through fx_time_steps"}
 
 
+def front_radii(d, sc, hdry: float) -> list:
+    """Largest distance from the dam's centre at which the depth exceeds
+    hdry, along 8 rays (every 45 degrees), sampled every quarter cell."""
+    h = d.download("h")[1:-1, 1:-1]  # [icol - 1, irow - 1]
+    n, dxy = sc.nrows, sc.dxy
+    out = []
+    for k in range(8):
+        a = k * np.pi / 4
+        r = np.arange(0.0, n * dxy / 2 * 1.5, dxy / 4)
+        x = n * dxy / 2 + r * np.cos(a)
+        y = n * dxy / 2 + r * np.sin(a)
+        ok = (x >= 0) & (x < n * dxy) & (y >= 0) & (y < n * dxy)
+        r, ix, iy = r[ok], (x[ok] // dxy).astype(int), (y[ok] // dxy).astype(int)
+        wet = h[iy, ix] > hdry
+        out.append(float(r[wet].max()) if wet.any() else 0.0)
+    return out
+
+
+def run_dambreak(args) -> dict:
+    """The circular dam break (2048^2 cells of 1 m, 2 m of water within 300 m
+    of the centre, flat bed, Manning n 0.02, two solutes, 600 s): FP32 against
+    FP64 at the horizon, with the front position along 8 rays and both water
+    balances."""
+    from fluxos_cpp_b200 import accuracy as A
+    from fluxos_cpp_b200 import scenarios as S
+    n = args.dambreak_size
+    sc = S.dambreak_scenario(n, dxy=1, radius=300.0 * n / 2048, depth=2.0, base=100.0,
+                             horizon=args.dambreak_horizon)
+    out = {"cells": n * n, "horizon_s": sc.horizon, "radius_m": sc.extra["radius"]}
+    doms, w0 = {}, {}
+    for p in ("fp64", "fp32"):
+        d = S.make_domain(sc, precision=p, steps_in_flight=31)
+        w0[p] = d.mass()[0]
+        t0 = time.perf_counter()
+        st = d.run_to_print()  # one output, at the horizon
+        out[f"{p}_steps"] = st["steps"]
+        out[f"{p}_wall_s"] = round(time.perf_counter() - t0, 3)
+        out[f"{p}_tim"] = st["tim"]
+        doms[p] = d
+    e = A.state_errors(doms["fp32"], doms["fp64"], sc.ks)
+    out["depth_l1_rel"] = e["depth"]["l1_rel"]
+    out["depth_linf_abs"] = e["depth"]["linf_abs"]
+    out["discharge_l1_rel"] = e["discharge"]["l1_rel"]
+    out["wet_cells_differ"] = e["wet_cells"]["differ"]
+    out["solute_mass_l1_rel"] = [c["l1_rel"] for c in e["solute_mass_density"]]
+    for p in ("fp64", "fp32"):
+        out[f"{p}_front_m"] = front_radii(doms[p], sc, sc.ks)
+        out[f"{p}_mass_rel_err"] = A.water_balance(doms[p], w0[p])["rel_err"]
+        doms[p].close()
+    return out
+
+
 def run_serve(args) -> dict:
     from fluxos_cpp_b200 import serve
     reqs = serve.poisson_requests(rate=4.0, duration=args.serve_seconds, seed=4,
@@ -419,6 +501,9 @@ def run_gpu(args):
                "note": "upload of the state from pinned host memory, the K steps through fx_step in "
                        "calls of steps-in-flight steps (each call reads the control block with every "
                        "step's record back), download of the Results fields; per-step bytes = totals / K"}
+    writer = None
+    if rank == 0 and world == 1 and not args.no_writer:
+        writer = results_writer_timing(doms[head])
     for d in doms.values():
         d.close()
     batches = (args.steps + k_batch - 1) // k_batch
@@ -427,6 +512,7 @@ def run_gpu(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_run(sc, h, conc, 1, args.cpu_steps, args.cpu_crop)
     mix = run_mix(args, peak) if (rank == 0 and world == 1 and not args.no_mix) else None
+    dam = run_dambreak(args) if (rank == 0 and world == 1 and not args.no_dambreak) else None
     srv = run_serve(args) if (rank == 0 and world == 1 and not args.no_serve) else None
     if rank == 0:
         roof = dict(res[head]["roofline"])
@@ -451,8 +537,12 @@ def run_gpu(args):
                             "autotuned": {"tile_rows": res["fp64"]["tile_rows"]},
                             "roofline": res["fp64"]["roofline"], "clocks": res["fp64"]["clocks"]}
             line["fp32_over_fp64"] = round(res[head]["value"] / res["fp64"]["value"], 3)
+        if writer is not None:
+            line["results_writer"] = writer
         if mix is not None:
             line["mix"] = mix
+        if dam is not None:
+            line["dambreak"] = dam
         if srv is not None:
             line["serve"] = srv
         print(json.dumps(line))
@@ -501,6 +591,10 @@ def main():
     ap.add_argument("--precision", default="both", choices=("both", "fp64", "fp32"),
                     help="both: FP32 headline with FP64 beside it and the FP32 error")
     ap.add_argument("--no-mix", action="store_true")
+    ap.add_argument("--no-writer", action="store_true", help="skip the Results writer timing")
+    ap.add_argument("--no-dambreak", action="store_true")
+    ap.add_argument("--dambreak-size", type=int, default=2048)
+    ap.add_argument("--dambreak-horizon", type=float, default=600.0)
     ap.add_argument("--mix-count", type=int, default=64)
     ap.add_argument("--mix-steps", type=int, default=62)
     ap.add_argument("--no-serve", action="store_true")

@@ -37,7 +37,8 @@ EXPORTED = ("fx_create", "fx_destroy", "fx_last_error", "fx_device_bytes", "fx_f
             "fx_batch_size", "fx_batch_step", "fx_batch_stream", "fx_batch_set_option",
             "fx_batch_autotune", "fx_adesolver_noalloc",
             "fx_initiate",
-            "fx_load_modset", "fx_open_modset", "fx_write_results", "fx_write_results_host", "fx_run")
+            "fx_load_modset", "fx_open_modset", "fx_write_results", "fx_write_results_async",
+            "fx_results_wait", "fx_write_results_host", "fx_run")
 
 
 class FluxosError(RuntimeError):
@@ -129,6 +130,8 @@ def lib() -> C.CDLL:
                                  dp, dp, fp, fp, fp, C.POINTER(ip)]
     L.fx_open_modset.argtypes = [cp, C.POINTER(vp)]
     L.fx_write_results.argtypes = [vp, cp]
+    L.fx_write_results_async.argtypes = [vp, cp]
+    L.fx_results_wait.argtypes = [vp]
     L.fx_write_results_host.argtypes = [cp, ip, ip, ip, C.c_double, C.c_double, C.c_double, dp, dp, dp,
                                         dp, dp, dp, dp, dp, dp, dp]
     L.fx_run.argtypes = [cp]
@@ -377,8 +380,19 @@ class Domain:
         self._ck(self.L.fx_mass(self.h, C.byref(w), _dptr(m)))
         return w.value, m[: self.nchem].copy()
 
-    def write_results(self, path: Optional[str] = None) -> None:
-        self._ck(self.L.fx_write_results(self.h, path.encode() if path else None))
+    def write_results(self, path: Optional[str] = None, wait: bool = True) -> None:
+        """The Results file of the current state (write_results.cpp:30-101),
+        by default <OUTPUT_FOLDER>/<print_next>.txt. With wait=False the rows
+        are compacted on the device and the file is written by a host thread
+        while the domain keeps stepping; results_wait() collects the outcome."""
+        p = path.encode() if path else None
+        if wait:
+            self._ck(self.L.fx_write_results(self.h, p))
+        else:
+            self._ck(self.L.fx_write_results_async(self.h, p))
+
+    def results_wait(self) -> None:
+        self._ck(self.L.fx_results_wait(self.h))
 
 
 class Batch:

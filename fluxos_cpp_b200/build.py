@@ -24,7 +24,7 @@ LIB = os.path.join(PKG, "lib")
 SO = os.path.join(LIB, "libfluxos_gpu.so")
 EXE = os.path.join(LIB, "fluxos_gpu")
 
-CU_SOURCES = ["fx_hydro.cu", "fx_ade.cu", "fx_capi.cu", "fx_batch.cu", "fx_noalloc.cu"]
+CU_SOURCES = ["fx_hydro.cu", "fx_ade.cu", "fx_capi.cu", "fx_batch.cu", "fx_noalloc.cu", "fx_results.cu"]
 CPP_SOURCES = ["fluxos_io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INC]

@@ -52,6 +52,7 @@ constexpr int RING = 4;       // per-lane prefetch slots (a power of two); a dee
                               // 8 slots made the FP64 sweep 2.5x slower)
 constexpr int DIST = 2;       // prefetch distance in columns (< RING)
 constexpr long long SPIN_LIMIT = 1LL << 20;  // polls (well under a second) before giving up
+constexpr long long HOLD_SPIN_LIMIT = 1LL << 12;  // the same with fx_dev.ade_hold (a test of the timeout path)
 
 // Per-lane ring of prefetched cells, filled by cp.async (asynchronous
 // global -> shared copies).
@@ -407,13 +408,18 @@ __device__ __forceinline__ bool dep_ok(const unsigned long long* p, unsigned lon
 
 // Wait until the counters reach the given warp-step counts; false if the wait
 // gave up (the error flag is then set).
+// With d.ade_hold set (fx_set_option "fail_ade_waits") a unit that has a
+// dependency never sees it met, so its wait runs out after HOLD_SPIN_LIMIT
+// polls: the timeout path, exercised without a fault.
 __device__ __forceinline__ bool wait_deps(const fx_dev& d, Deps& D, int need_w, int need_p0, int need_p1) {
   long long it = 0;
+  const bool hold = d.ade_hold != 0;
+  const long long limit = hold ? HOLD_SPIN_LIMIT : SPIN_LIMIT;
   for (;;) {
     const bool ok = dep_ok(D.w, D.seen_w, D.tag_w, need_w) && dep_ok(D.p0, D.seen_p0, D.tag_p, need_p0) &&
-                    dep_ok(D.p1, D.seen_p1, D.tag_p, need_p1);
+                    dep_ok(D.p1, D.seen_p1, D.tag_p, need_p1) && (!hold || (!D.w && !D.p0 && !D.p1));
     if (__all_sync(0xffffffffu, ok)) return true;
-    const bool stop = (++it > SPIN_LIMIT) || (*(volatile int*)&d.ctl->error != 0);
+    const bool stop = (++it > limit) || (*(volatile int*)&d.ctl->error != 0);
     if (__any_sync(0xffffffffu, stop)) {
       if ((threadIdx.x & 31) == 0) atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
       return false;

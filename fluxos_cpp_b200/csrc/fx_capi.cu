@@ -393,6 +393,7 @@ fail:
 
 void fx_destroy(fx_ctx* c) {
   if (!c) return;
+  fx_results_release(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   for (void* p : c->allocs) cudaFree(p);
@@ -681,6 +682,13 @@ int fx_set_option(fx_ctx* c, const char* name, long long v) {
     return FX_OK;
   }
   if (!strcmp(name, "tile_rows")) return set_tile_rows(c, (int)v);
+  if (!strcmp(name, "fail_ade_waits")) {
+    c->d.ade_hold = v != 0 ? 1 : 0;
+    c->graph_dirty = true;
+    c->dev_dirty = true;
+    c->dev_version++;
+    return FX_OK;
+  }
   if (!strcmp(name, "tma")) {
     c->use_tma = v != 0;
     c->graph_dirty = true;
@@ -795,6 +803,10 @@ int fx_step(fx_ctx* c, int nsteps, fx_status* st) {
   }
   int rc = read_ctl(c);
   if (rc) return rc;
+  if (c->ctl_host->error) {  // a kernel gave up a wait: the state is not stepped further
+    fx_fill_status(*c->ctl_host, st);
+    return status_rc(c);
+  }
   if ((rc = set_stop(c, c->ctl_host->steps + nsteps))) return rc;
   if ((rc = ensure_graph(c))) return rc;
   int left = nsteps;

@@ -142,7 +142,7 @@ struct fx_dev {
   // pair without rounding loss, and the wet/dry threshold tests compare
   // eta + eta_lo in FP64. zb stays FP64 for output.
   int prec32;
-  int pad4_;
+  int ade_hold;  // failure-detection test: the ADE sweep's dependency waits are never satisfied
   float *eta, *eta_lo, *qx_f, *qy_f, *twet_f;
   float *h_f, *h0_f, *hpm_f, *fe1_f, *fn1_f;  // nslot planes each
   float *fe2_f, *fe3_f, *fn2_f, *fn3_f;

@@ -45,9 +45,14 @@ struct fx_ctx {
   // file surface (filled by fx_open_modset)
   double h_min_print = 0.0;
   std::string output_folder;
+  // Results writer state (fluxos_io.cpp): device scratch of the row
+  // compaction, pinned buffers and the writer threads; released by
+  // fx_results_release
+  struct fx_results_state* res = nullptr;
 };
 
 int fx_fail(fx_ctx* ctx, int code, const char* fmt, ...);
+void fx_results_release(fx_ctx* ctx);  // waits for pending Results files, frees the writer's buffers
 int fx_sync_dev(fx_ctx* ctx);
 void fx_fill_status(const fx_ctl& k, fx_status* st);
 
@@ -67,6 +72,15 @@ void fx_launch_ade_one(const fx_dev& d, int nunits, int nblocks, cudaStream_t s)
 void fx_launch_eta_from_z(const fx_dev& d, const double* z, cudaStream_t s);
 void fx_launch_mass(const fx_dev& d, double* out, cudaStream_t s);
 void fx_tiles_of(int dom, int nr, int nc, int tile_rows, std::vector<fx_tile>& out);
+// Results rows on the device (fx_results.cu): per-column counts (nc
+// unsigned) and their exclusive scan (nc + 1 long long, the total last);
+// then the rows as column arrays in `buf`: irow, icol (int32) and
+// FX_RES_NVAL FP64 columns, `total` entries each.
+#define FX_RES_NVAL 9
+void fx_launch_results_count(const fx_dev& d, double h_min_print, unsigned* counts, long long* offs,
+                             cudaStream_t s);
+void fx_launch_results_write(const fx_dev& d, double h_min_print, const long long* offs, void* buf,
+                             long long total, cudaStream_t s);
 bool fx_tile_rows_ok(int tile_rows);
 void fx_units_of(int dom, int nr, int nchem, int steps, std::vector<fx_unit>& out);
 int fx_ade_rows_per_strip();

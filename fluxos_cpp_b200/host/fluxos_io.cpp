@@ -17,6 +17,7 @@
 //     length is the last row's time truncated to an integer (main.cpp:181-192).
 #include <algorithm>
 #include <cctype>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -28,6 +29,7 @@
 #include <sstream>
 #include <string>
 #include <sys/stat.h>
+#include <thread>
 #include <vector>
 
 #include "../csrc/fx_internal.h"
@@ -618,13 +620,181 @@ int upload_state(fx_ctx* c, const InitState& s) {
   return fx_upload_flags(c, s.ldry.data(), s.wall.data());
 }
 
-std::string fmt17(double v) {
+// Appends v as printf's "%.17g" writes it (std::to_chars with the general
+// format and precision 17 is specified to give the same characters).
+inline void put17(std::string& out, double v) {
   char buf[40];
-  snprintf(buf, sizeof(buf), "%.17g", v);
-  return buf;
+  const auto r = std::to_chars(buf, buf + sizeof(buf), v, std::chars_format::general, 17);
+  out.append(buf, r.ptr);
+}
+
+// One Results row (write_results.cpp:48-80): irow, icol, X, Y, z, z - zb,
+// ux, uy, qx * dxy, qy * dxy, us, conc, soil_mass, fe_1, fn_1, twet, where
+// ux, uy and us are 0 (never computed by the reference).
+inline void put_row(std::string& out, int irow, int icol, int dxy, double xll, double yll, const double* v9) {
+  const double row[16] = {(double)irow, (double)icol,
+                          (double)((unsigned long)icol * (unsigned long)dxy) + xll,
+                          (double)((unsigned long)irow * (unsigned long)dxy) + yll,
+                          v9[0], v9[1], 0.0, 0.0, v9[2], v9[3], 0.0, v9[4], v9[5], v9[6], v9[7], v9[8]};
+  for (int k = 0; k < 16; ++k) {
+    put17(out, row[k]);
+    out += (k < 15) ? ',' : '\n';
+  }
+}
+
+const char* const kResultsHeader =
+    "irow [-],icol [-],Xcoord,Ycoord,z [m],h [m],ux [m/s],uy [m/s],qx * dxy [m3/sec],"
+    "qy * dxy [m3/sec],us [m/s],conc_SW [mg/l],soil_mass [g],fe_1 [m2/s],fn_1 [m2/s],"
+    "twetimetracer [sec]\n";
+
+// Rows as the device packs them (fx_results.cu): irow, icol, then
+// FX_RES_NVAL columns of `n` values.
+struct PackedRows {
+  const int* irow;
+  const int* icol;
+  const double* v[FX_RES_NVAL];
+  long long n;
+};
+
+PackedRows unpack(const void* buf, long long n) {
+  PackedRows r;
+  const char* p = (const char*)buf;
+  r.irow = (const int*)p;
+  r.icol = (const int*)(p + 4 * n);
+  for (int k = 0; k < FX_RES_NVAL; ++k) r.v[k] = (const double*)(p + 8 * n + 8 * n * k);
+  r.n = n;
+  return r;
+}
+
+// Writes a Results file from packed rows: the text of blocks of rows is
+// formatted by several threads, then written in order. With no row the
+// reference still writes one row of zeros (write_results.cpp:309-310 keeps
+// span(0, max(0, a-1))).
+int write_packed(const std::string& path, const PackedRows& r, int dxy, double xll, double yll,
+                 std::string& err) {
+  FILE* fp = fopen(path.c_str(), "w");
+  if (!fp) {
+    err = "cannot write " + path;
+    return FX_ERR_IO;
+  }
+  fputs(kResultsHeader, fp);
+  if (r.n == 0) {
+    for (int k = 0; k < 16; ++k) fputs(k < 15 ? "0," : "0\n", fp);
+  } else {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const long long per = 16384;  // rows per thread and block
+    const int nt = (int)std::min<long long>(hw, (r.n + per - 1) / per);
+    std::vector<std::string> text(nt);
+    for (long long base = 0; base < r.n; base += per * nt) {
+      auto work = [&](int t) {
+        std::string& out = text[t];
+        out.clear();
+        const long long a = base + per * t, b = std::min(r.n, a + per);
+        double v9[FX_RES_NVAL];
+        for (long long i = a; i < b; ++i) {
+          for (int k = 0; k < FX_RES_NVAL; ++k) v9[k] = r.v[k][i];
+          put_row(out, r.irow[i], r.icol[i], dxy, xll, yll, v9);
+        }
+      };
+      std::vector<std::thread> th;
+      for (int t = 1; t < nt; ++t) th.emplace_back(work, t);
+      work(0);
+      for (auto& x : th) x.join();
+      for (int t = 0; t < nt; ++t) fwrite(text[t].data(), 1, text[t].size(), fp);
+    }
+  }
+  if (fclose(fp) != 0) {
+    err = "cannot write " + path;
+    return FX_ERR_IO;
+  }
+  return FX_OK;
 }
 
 }  // namespace
+
+// Results writer state of a context. Each file goes through one of two
+// slots: the rows are compacted on the context's stream, copied to the
+// slot's pinned buffer on a copy stream, and formatted and written by the
+// slot's thread while the context keeps stepping.
+struct fx_results_state {
+  struct Slot {
+    std::thread th;
+    void* host = nullptr;  // pinned
+    size_t cap = 0;
+    cudaEvent_t copied = nullptr;
+    int rc = FX_OK;
+    std::string err;
+  };
+  Slot slot[2];
+  int next = 0;
+  cudaStream_t copy = nullptr;
+  unsigned* counts = nullptr;   // device, nc
+  long long* offs = nullptr;    // device, nc + 1
+  void* rows = nullptr;         // device packed rows
+  size_t rows_cap = 0;
+  long long* total_host = nullptr;  // pinned
+  cudaEvent_t rows_free = nullptr;  // the last copy out of `rows` is done
+};
+
+namespace {
+
+int res_cuda(fx_ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return FX_OK;
+  return fx_fail(c, FX_ERR_CUDA, "%s failed: %s", what, cudaGetErrorString(e));
+}
+
+// Joins the slot's writer thread; returns its outcome.
+int res_join(fx_ctx* c, fx_results_state::Slot& sl) {
+  if (sl.th.joinable()) sl.th.join();
+  const int rc = sl.rc;
+  if (rc) fx_fail(c, rc, "%s", sl.err.c_str());
+  sl.rc = FX_OK;
+  sl.err.clear();
+  return rc;
+}
+
+int res_init(fx_ctx* c) {
+  if (c->res) return FX_OK;
+  auto* r = new fx_results_state();
+  c->res = r;
+  int rc;
+  if ((rc = res_cuda(c, cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking), "cudaStreamCreate")) ||
+      (rc = res_cuda(c, cudaMalloc((void**)&r->counts, sizeof(unsigned) * (size_t)c->d.nc), "cudaMalloc")) ||
+      (rc = res_cuda(c, cudaMalloc((void**)&r->offs, sizeof(long long) * ((size_t)c->d.nc + 1)), "cudaMalloc")) ||
+      (rc = res_cuda(c, cudaMallocHost((void**)&r->total_host, sizeof(long long)), "cudaMallocHost")) ||
+      (rc = res_cuda(c, cudaEventCreateWithFlags(&r->rows_free, cudaEventDisableTiming), "cudaEventCreate")))
+    return rc;
+  for (auto& sl : r->slot)
+    if ((rc = res_cuda(c, cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming), "cudaEventCreate")))
+      return rc;
+  return FX_OK;
+}
+
+}  // namespace
+
+void fx_results_release(fx_ctx* c) {
+  if (!c || !c->res) return;
+  fx_results_state* r = c->res;
+  for (auto& sl : r->slot) {
+    if (sl.th.joinable()) sl.th.join();
+    if (sl.copied) cudaEventDestroy(sl.copied);
+    if (sl.host) cudaFreeHost(sl.host);
+  }
+  if (r->copy) {
+    cudaStreamSynchronize(r->copy);
+    cudaStreamDestroy(r->copy);
+  }
+  if (r->rows_free) cudaEventDestroy(r->rows_free);
+  if (r->rows) {
+    cudaFree(r->rows);
+    c->bytes -= (long long)r->rows_cap;
+  }
+  if (r->counts) cudaFree(r->counts);
+  if (r->offs) cudaFree(r->offs);
+  if (r->total_host) cudaFreeHost(r->total_host);
+  delete r;
+  c->res = nullptr;
+}
 
 extern "C" {
 
@@ -821,64 +991,120 @@ int fx_write_results_host(const char* path, int nrows, int ncols, int dxy, doubl
                           const double* twet) {
   if (!path || !z || !zb || !h || !qx || !qy || !conc || !fe1 || !fn1 || !twet)
     return fx_fail(nullptr, FX_ERR_ARG, "fx_write_results_host: null argument");
-  FILE* fp = fopen(path, "w");
-  if (!fp) return fx_fail(nullptr, FX_ERR_IO, "cannot write %s", path);
-  // write_results.cpp:312-330: header of 16 names, then the selected rows.
-  fputs("irow [-],icol [-],Xcoord,Ycoord,z [m],h [m],ux [m/s],uy [m/s],qx * dxy [m3/sec],"
-        "qy * dxy [m3/sec],us [m/s],conc_SW [mg/l],soil_mass [g],fe_1 [m2/s],fn_1 [m2/s],"
-        "twetimetracer [sec]\n",
-        fp);
+  // write_results.cpp:44-80: the selected cells (zb != 0, h > H_MIN_TO_PRINT)
+  // in column-major order, packed as the device packs them
   const size_t mr = (size_t)nrows + 2;
   const double dx = (double)dxy;
-  long long rows = 0;
-  std::string line;
+  std::vector<int> ir, ic;
+  std::vector<double> vals[FX_RES_NVAL];
   for (int icol = 1; icol <= ncols; icol++) {
     for (int irow = 1; irow <= nrows; irow++) {
       const size_t i = (size_t)icol * mr + (size_t)irow;
-      if (zb[i] != 0.0 && h[i] > h_min_print) {  // :280
-        const double v[16] = {(double)irow, (double)icol, (double)((unsigned long)icol * (unsigned long)dxy) + xll,
-                              (double)((unsigned long)irow * (unsigned long)dxy) + yll, z[i], z[i] - zb[i], 0.0,
-                              0.0, qx[i] * dx, qy[i] * dx, 0.0, conc[i], soil_mass ? soil_mass[i] : 0.0,
-                              fe1[i], fn1[i], twet[i]};
-        line.clear();
-        for (int k = 0; k < 16; ++k) {
-          line += fmt17(v[k]);
-          line += (k < 15) ? ',' : '\n';
-        }
-        fputs(line.c_str(), fp);
-        ++rows;
+      if (zb[i] != 0.0 && h[i] > h_min_print) {
+        const double v9[FX_RES_NVAL] = {z[i], z[i] - zb[i], qx[i] * dx, qy[i] * dx, conc[i],
+                                        soil_mass ? soil_mass[i] : 0.0, fe1[i], fn1[i], twet[i]};
+        ir.push_back(irow);
+        ic.push_back(icol);
+        for (int k = 0; k < FX_RES_NVAL; ++k) vals[k].push_back(v9[k]);
       }
     }
   }
-  // With no selected cell the reference still writes one row of zeros
-  // (write_results.cpp:309-310 keeps span(0, max(0, a-1))).
-  if (rows == 0)
-    for (int k = 0; k < 16; ++k) fputs(k < 15 ? "0," : "0\n", fp);
-  if (fclose(fp) != 0) return fx_fail(nullptr, FX_ERR_IO, "cannot write %s", path);
+  PackedRows r;
+  r.irow = ir.data();
+  r.icol = ic.data();
+  for (int k = 0; k < FX_RES_NVAL; ++k) r.v[k] = vals[k].data();
+  r.n = (long long)ir.size();
+  std::string err;
+  const int rc = write_packed(path, r, dxy, xll, yll, err);
+  if (rc) return fx_fail(nullptr, rc, "%s", err.c_str());
   return FX_OK;
+}
+
+int fx_write_results_async(fx_ctx* c, const char* path) {
+  if (!c) return FX_ERR_ARG;
+  int rc;
+  if (c->d.prec32 && !c->z_pending.empty() && (rc = fx_prepare(c))) return rc;
+  fx_status st;
+  if ((rc = fx_get_status(c, &st))) return rc;
+  std::string fn;
+  if (path) fn = path;
+  else fn = c->output_folder + "/" + std::to_string((long long)std::llround(st.print_next)) + ".txt";
+  if ((rc = res_init(c)) || (rc = fx_sync_dev(c))) return rc;
+  fx_results_state& r = *c->res;
+  fx_results_state::Slot& sl = r.slot[r.next];
+  r.next ^= 1;
+  if ((rc = res_join(c, sl))) return rc;  // the slot's previous file
+  // count and place the selected cells, then size the buffers
+  fx_launch_results_count(c->d, c->h_min_print, r.counts, r.offs, c->stream);
+  if ((rc = res_cuda(c, cudaMemcpyAsync(r.total_host, r.offs + c->d.nc, sizeof(long long),
+                                        cudaMemcpyDeviceToHost, c->stream), "cudaMemcpyAsync")) ||
+      (rc = res_cuda(c, cudaStreamSynchronize(c->stream), "results count")))
+    return rc;
+  const long long total = *r.total_host;
+  const size_t bytes = (size_t)total * (8 + 8 * FX_RES_NVAL);
+  if (bytes > r.rows_cap) {
+    if ((rc = res_cuda(c, cudaEventSynchronize(r.rows_free), "cudaEventSynchronize"))) return rc;
+    if (r.rows) {
+      cudaFree(r.rows);
+      c->bytes -= (long long)r.rows_cap;
+      r.rows = nullptr;
+      r.rows_cap = 0;
+    }
+    if ((rc = res_cuda(c, cudaMalloc(&r.rows, bytes), "cudaMalloc (Results rows)"))) return rc;
+    r.rows_cap = bytes;
+    c->bytes += (long long)bytes;
+  }
+  if (bytes > sl.cap) {
+    if (sl.host) cudaFreeHost(sl.host);
+    sl.host = nullptr;
+    sl.cap = 0;
+    if ((rc = res_cuda(c, cudaMallocHost(&sl.host, bytes), "cudaMallocHost (Results rows)"))) return rc;
+    sl.cap = bytes;
+  }
+  // the previous file's copy out of the row buffer must be done first
+  if ((rc = res_cuda(c, cudaStreamWaitEvent(c->stream, r.rows_free, 0), "cudaStreamWaitEvent"))) return rc;
+  if (total > 0) fx_launch_results_write(c->d, c->h_min_print, r.offs, r.rows, total, c->stream);
+  if ((rc = res_cuda(c, cudaGetLastError(), "results kernels")) ||
+      (rc = res_cuda(c, cudaEventRecord(sl.copied, c->stream), "cudaEventRecord")) ||
+      (rc = res_cuda(c, cudaStreamWaitEvent(r.copy, sl.copied, 0), "cudaStreamWaitEvent")))
+    return rc;
+  if (total > 0 && (rc = res_cuda(c, cudaMemcpyAsync(sl.host, r.rows, bytes, cudaMemcpyDeviceToHost, r.copy),
+                                  "cudaMemcpyAsync (Results rows)")))
+    return rc;
+  if ((rc = res_cuda(c, cudaEventRecord(sl.copied, r.copy), "cudaEventRecord")) ||
+      (rc = res_cuda(c, cudaEventRecord(r.rows_free, r.copy), "cudaEventRecord")))
+    return rc;
+  const int dxy = c->g.dxy;
+  const double xll = c->g.xll, yll = c->g.yll;
+  fx_results_state::Slot* sp = &sl;
+  sl.th = std::thread([sp, fn, total, dxy, xll, yll]() {
+    const cudaError_t e = cudaEventSynchronize(sp->copied);
+    if (e != cudaSuccess) {
+      sp->rc = FX_ERR_CUDA;
+      sp->err = std::string("Results copy failed: ") + cudaGetErrorString(e);
+      return;
+    }
+    sp->rc = write_packed(fn, unpack(sp->host, total), dxy, xll, yll, sp->err);
+  });
+  return FX_OK;
+}
+
+int fx_results_wait(fx_ctx* c) {
+  if (!c) return FX_ERR_ARG;
+  if (!c->res) return FX_OK;
+  int first = FX_OK;
+  for (auto& sl : c->res->slot) {
+    const int rc = res_join(c, sl);
+    if (rc && !first) first = rc;
+  }
+  return first;
 }
 
 int fx_write_results(fx_ctx* c, const char* path) {
   if (!c) return FX_ERR_ARG;
-  fx_status st;
-  int rc = fx_get_status(c, &st);
-  if (rc) return rc;
-  std::string fn;
-  if (path) fn = path;
-  else fn = c->output_folder + "/" + std::to_string((long long)std::llround(st.print_next)) + ".txt";
-  const size_t n = ((size_t)c->g.nrows + 2) * ((size_t)c->g.ncols + 2);
-  std::vector<double> z(n), zb(n), h(n), qx(n), qy(n), cc(n), sm(n), fe(n), fnn(n), tw(n);
-  if ((rc = fx_download(c, "z", z.data())) || (rc = fx_download(c, "zb", zb.data())) ||
-      (rc = fx_download(c, "h", h.data())) || (rc = fx_download(c, "qx", qx.data())) ||
-      (rc = fx_download(c, "qy", qy.data())) || (rc = fx_download(c, "conc", cc.data())) ||
-      (rc = fx_download(c, "soil_mass", sm.data())) || (rc = fx_download(c, "fe_1", fe.data())) ||
-      (rc = fx_download(c, "fn_1", fnn.data())) || (rc = fx_download(c, "twet", tw.data())))
-    return rc;
-  rc = fx_write_results_host(fn.c_str(), c->g.nrows, c->g.ncols, c->g.dxy, c->g.xll, c->g.yll,
-                             c->h_min_print, z.data(), zb.data(), h.data(), qx.data(), qy.data(), cc.data(),
-                             sm.data(), fe.data(), fnn.data(), tw.data());
-  if (rc) c->err = fx_last_error(nullptr);
-  return rc;
+  int rc = fx_write_results_async(c, path);
+  const int rw = fx_results_wait(c);
+  return rc ? rc : rw;
 }
 
 int fx_run(const char* modset_path) {
@@ -890,15 +1116,18 @@ int fx_run(const char* modset_path) {
     rc = fx_run_to_print(c, &st);
     if (rc) break;
     if (st.print_pending) {
-      if ((rc = fx_write_results(c, nullptr))) break;
+      if ((rc = fx_write_results_async(c, nullptr))) break;  // written while the next steps run
       printf("Saved: '%lld.txt'\n", (long long)std::llround(st.print_next));
       if ((rc = fx_print_done(c))) break;
       continue;
     }
     if (st.finished) break;
   }
+  const int rw = fx_results_wait(c);
+  if (!rc) rc = rw;
   fx_destroy(c);
   return rc;
 }
+
 
 }  // extern "C"

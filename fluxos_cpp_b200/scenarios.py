@@ -344,6 +344,7 @@ def make_domain(sc: Scenario, *, precision: str = "fp64", steps_in_flight: int =
     import fluxos_cpp_b200 as fx
     d = fx.Domain(sc.nrows, sc.ncols, sc.dxy, nchem=sc.nchem, nodata=float(sc.nodata), hdry=sc.ks,
                   ntim=sc.horizon, print_step=sc.print_step, print_next=sc.print_step, ade=sc.ade,
+                  h_min_print=float(sc.h_min_print),
                   d_coef=list(sc.d_coefs) if sc.d_coefs else [sc.d_coef],
                   steps_in_flight=steps_in_flight, precision=precision, wintra=sc.wintra,
                   soil_release_rate=sc.soil_release_rate)

@@ -143,7 +143,12 @@ int fx_set_melt_field(fx_ctx* ctx, const double* mult_grid);
  * 32 x tile_rows threads; default 8); "tma" (1, the default: a persistent
  * hydrodynamic kernel whose blocks stage each tile's stencil into shared
  * memory by TMA while computing the previous tile; 0: one block per tile
- * loading its stencil itself). Results depend on neither. */
+ * loading its stencil itself). Results depend on neither.
+ * "fail_ade_waits" (1: for testing failure detection, the ADE sweep's
+ * dependency waits are never satisfied, so they give up after a few
+ * thousand polls, the kernels return, and the step returns FX_ERR_DEVICE
+ * with fx_status.device_error set; the context then refuses further steps
+ * and stays destroyable, the device stays usable). */
 int fx_set_option(fx_ctx* ctx, const char* name, long long value);
 int fx_prepare(fx_ctx* ctx);
 
@@ -244,6 +249,17 @@ int fx_open_modset(const char* modset_path, fx_ctx** out);
 /* write_results (write_results.cpp:30-101): Results/<t>.txt of the current
  * state; path NULL means <OUTPUT_FOLDER>/<print_next>.txt. */
 int fx_write_results(fx_ctx* ctx, const char* path);
+/* The same file written while the context keeps stepping: the selected
+ * rows are compacted on the device (cells with zb != 0 and h >
+ * H_MIN_TO_PRINT, in the file's order) on the context's stream, copied to
+ * pinned memory on a second stream, and formatted and written by a host
+ * thread. Returns once the rows are placed; the state may then be stepped.
+ * fx_results_wait waits for every file started and returns the first error
+ * (FX_ERR_IO when a file could not be written); fx_destroy waits too. The
+ * row buffer (80 bytes per printed cell) is held on the device until
+ * fx_destroy and is counted by fx_device_bytes, not by fx_footprint. */
+int fx_write_results_async(fx_ctx* ctx, const char* path);
+int fx_results_wait(fx_ctx* ctx);
 /* The writer itself on host grids (no GPU needed); soil_mass may be NULL
  * (a column of zeros). */
 int fx_write_results_host(const char* path, int nrows, int ncols, int dxy, double xll, double yll,

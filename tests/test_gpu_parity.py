@@ -220,3 +220,30 @@ def test_wintra_soil_release_parity(in_flight, nchem, tmp_path):
         assert not bad, (n, bad)
     assert ora.grid("soil_mass").sum() < 0.999 * soil0  # the release happened
     d.close()
+
+
+def test_bounded_wait_timeout_reports_device_error(tmp_path):
+    """Failure detection without a fault: with the ADE dependency waits held
+    unsatisfied (option fail_ade_waits), the waits run out, the step returns
+    FX_ERR_DEVICE with the status flag set, the context refuses to step on,
+    and a new context on the same device runs normally."""
+    sc = _random_scenario(120, 90, 61)
+    sc.write(str(tmp_path))
+    ora = P.OracleRun(str(tmp_path), sc, 0)
+    h = np.random.default_rng(2).uniform(0, 0.02, (120, 90))
+    ora.apply_wet_start(h, None, None, [np.where(h > 0.01, 1.0, 0.0)])
+    d = GP.domain_from_oracle(ora, sc, 0, steps_in_flight=8)
+    d.set_option("fail_ade_waits", 1)
+    with pytest.raises(fx.FluxosError) as e:
+        d.step(8)
+    assert e.value.code == -5 and "bounded wait" in str(e.value)
+    assert d.status()["device_error"] != 0
+    with pytest.raises(fx.FluxosError):
+        d.step(1)
+    d.close()
+    d2 = GP.domain_from_oracle(ora, sc, 0, steps_in_flight=8)
+    GP.advance_oracle(ora, 20)
+    GP.advance_domain(d2, 20)
+    res, bad = GP.compare(ora, d2, sc)
+    assert not bad, bad
+    d2.close()
