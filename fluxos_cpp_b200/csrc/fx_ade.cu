@@ -658,8 +658,25 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
 
 // One domain: the descriptor is a kernel parameter. Unit u is strip
 // u % nstrips of solute (u / nstrips) % nchem at step u / (nstrips * nchem).
+// Resident blocks per SM the sweep kernels are compiled for (3: 168
+// registers in FP64, 152 in FP32). More resident warps do not pay: their
+// rings take shared memory from L1, which serves the lanes' skewed reads
+// (FP32 at 4096 x 4096: 1.17 ms per step with 3 blocks, 1.45 with 4 at 128
+// registers, 1.41 with 5).
+#ifndef FX_ADE_F32_BLOCKS
+#define FX_ADE_F32_BLOCKS 3
+#endif
 template <class T>
-__global__ void __launch_bounds__(WARPS * 32, 3) k_ade_one(const __grid_constant__ fx_dev d,
+struct AdeBlocks {
+  static constexpr int value = 3;
+};
+template <>
+struct AdeBlocks<float> {
+  static constexpr int value = FX_ADE_F32_BLOCKS;
+};
+
+template <class T>
+__global__ void __launch_bounds__(WARPS * 32, AdeBlocks<T>::value) k_ade_one(const __grid_constant__ fx_dev d,
                                                                            int nunits) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
@@ -677,7 +694,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_ade_one(const __grid_constant
 // A batch of domains: units come from the unit table; each warp copies its
 // unit's descriptor to its own shared-memory slot.
 template <class T>
-__global__ void __launch_bounds__(WARPS * 32, 3) k_ade_batch(const fx_dev* __restrict__ devs,
+__global__ void __launch_bounds__(WARPS * 32, AdeBlocks<T>::value) k_ade_batch(const fx_dev* __restrict__ devs,
                                                          const fx_unit* __restrict__ units, int nunits) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ fx_dev wdev[WARPS];
