@@ -448,8 +448,9 @@ def run_dambreak(args) -> dict:
         d.close()
     out["note"] = ("the initial concentration is at most 1; the reference's ADE scheme (restated "
                    "bit for bit by the FP64 path) is not bounded at D = 1.0 m^2/s on 1 m cells: "
-                   "its concentrations grow by orders of magnitude, so solute errors between the "
-                   "precisions compare two unstable runs")
+                   "the second solute's concentrations grow by orders of magnitude and then "
+                   "collapse to ~0, so solute errors between the precisions compare two "
+                   "unstable runs")
     return out
 
 

@@ -1444,10 +1444,14 @@ __device__ __forceinline__ void hydro_block(const fx_dev& d, const fx_tile& tile
   else hydro_tile64<BY>(d, c, tile, S);
 }
 
-// Blocks per SM the launch bounds ask for: 512 threads for FP64 (at most 128
-// registers each), 768 for FP32 (at most 85).
+// Blocks per SM the launch bounds ask for: 768 threads for FP64 (at most 85
+// registers each), 1024 for FP32 (at most 64). The kernel is bound by
+// instruction latency and tile barriers, so resident warps pay for the
+// spills this costs: at 4096 x 4096 cells the FP32 kernel took 1.50 ms per
+// step at 64 registers against 1.73 ms at 80 (3 blocks), the FP64 one 4.01
+// ms at 85 against 4.39 ms at 128 (2 blocks).
 template <bool P32, int BY>
-constexpr int min_blocks() { return (P32 ? 24 : 16) / BY > 0 ? (P32 ? 24 : 16) / BY : 1; }
+constexpr int min_blocks() { return (P32 ? 32 : 24) / BY > 0 ? (P32 ? 32 : 24) / BY : 1; }
 
 // One domain: the descriptor is a kernel parameter (constant bank), so its
 // fields are instruction operands. Block (x, y) is tile (x, y).
