@@ -69,8 +69,8 @@ ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
 # case of this workload, one launch, divided by the cells and the steps the
 # launch covers); traffic scales with the cells, so `traffic` in the line is
 # this times the cells of the run.
-DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 125.95, "k_ade_sweep": 61.35},
-                       "fp32": {"k_hydro": 72.40, "k_ade_sweep": 25.33}}
+DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 149.33, "k_ade_sweep": 61.35},
+                       "fp32": {"k_hydro": 80.10, "k_ade_sweep": 25.33}}
 
 
 def _rank():
@@ -282,11 +282,16 @@ def cpu_reference_run(sc, h, conc, warmup: int, steps: int, crop: int):
                       f"serial ADE"}
 
 
-def measure_domain(d, steps: int, warmup: int, cells: int, precision: str, peak: float, gpu: str):
-    """Autotune the tile shape (real steps, part of the warm-up), warm-up,
-    then `steps` timed steps (CUDA events on the domain's stream around every
-    launch, fx_time_steps); roofline of the dominant kernel."""
-    tile_rows = d.autotune(8)
+def measure_domain(d, steps: int, warmup: int, cells: int, precision: str, peak: float, gpu: str,
+                   tile_rows: int = 0):
+    """Autotune the tile shape (real steps, part of the warm-up) unless one is
+    given, warm-up, then `steps` timed steps (CUDA events on the domain's
+    stream around every launch, fx_time_steps); roofline of the dominant
+    kernel."""
+    if tile_rows:
+        d.set_option("tile_rows", tile_rows)
+    else:
+        tile_rows = d.autotune(8)
     d.step(warmup)
     sampler = ClockSampler(gpu)
     sampler.start()
@@ -493,7 +498,7 @@ def run_gpu(args):
         dist.barrier()
     torch.cuda.synchronize()
     for p in precs:
-        res[p] = measure_domain(doms[p], args.steps, args.warmup, cells, p, peak, gpu)
+        res[p] = measure_domain(doms[p], args.steps, args.warmup, cells, p, peak, gpu, args.tile_rows)
     torch.cuda.synchronize()
     head = precs[0]
     t = torch.tensor([res[head]["ms_total"]], dtype=torch.float64, device="cuda")
@@ -605,6 +610,8 @@ def main():
     ap.add_argument("--no-mix", action="store_true")
     ap.add_argument("--no-writer", action="store_true", help="skip the Results writer timing")
     ap.add_argument("--no-dambreak", action="store_true")
+    ap.add_argument("--tile-rows", type=int, default=0, choices=(0, 4, 8, 16),
+                    help="hydrodynamic tile shape (0: autotune)")
     ap.add_argument("--dambreak-size", type=int, default=2048)
     ap.add_argument("--dambreak-horizon", type=float, default=600.0)
     ap.add_argument("--mix-count", type=int, default=64)
