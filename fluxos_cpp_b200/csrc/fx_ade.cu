@@ -46,7 +46,7 @@ namespace fxade {
 
 constexpr int ROWS = 30;      // rows per strip (lanes 0..29 compute)
 constexpr int WARPS = 4;      // warps per block
-constexpr int CHUNK = 4;      // steps between progress checks and publications
+constexpr int CHUNK = 8;      // steps between progress checks and publications
 constexpr int RING = 4;       // per-lane prefetch slots (a power of two); a deeper ring takes shared
                               // memory from L1, which the lanes' skewed reads depend on (measured:
                               // 8 slots made the FP64 sweep 2.5x slower)
@@ -745,12 +745,35 @@ void fx_units_of(int dom, int nr, int nchem, int steps, std::vector<fx_unit>& ou
       for (int s = 0; s < nstrips; ++s) out.push_back(fx_unit{dom, jj, k, s});
 }
 
+// Resident blocks per SM of a sweep kernel. The kernel then asks for the
+// smallest shared-memory carveout that still holds that many blocks: the
+// rest of the SM's on-chip memory is L1, which serves the lanes' skewed
+// reads. The count is queried again under the carveout, and the carveout
+// is dropped if it would hold fewer blocks.
 template <class K>
 static int max_blocks_of(K kernel, size_t smem, int nsm, int* out) {
   int per = 0;
   if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, fxade::WARPS * 32, smem) != cudaSuccess)
     return -1;
+  int dev = 0, sm_max = 0, reserved = 0;
+  cudaFuncAttributes fa;
+  if (per > 0 && cudaGetDevice(&dev) == cudaSuccess &&
+      cudaDeviceGetAttribute(&sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess &&
+      cudaFuncGetAttributes(&fa, kernel) == cudaSuccess && sm_max > 0) {
+    const long long need = (long long)per * ((long long)smem + (long long)fa.sharedSizeBytes + reserved);
+    const int pct = (int)std::min<long long>(100, (need * 100 + sm_max - 1) / sm_max);
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct) == cudaSuccess) {
+      int per2 = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, kernel, fxade::WARPS * 32, smem) != cudaSuccess)
+        return -1;
+      if (per2 < per &&
+          cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, -1) != cudaSuccess)
+        return -1;
+    }
+  }
+  cudaGetLastError();  // a refused hint leaves no error behind
   *out = per * nsm;
   return 0;
 }
