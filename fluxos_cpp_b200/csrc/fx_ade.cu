@@ -229,9 +229,13 @@ __device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, con
     if (S.dilute && !(fl & FX_F_NODATA)) {
       const T hp = R.hp[slot][lane];
       if (hp != T(0)) {
-        const T mi = Fields<T>::mm(d)
-                         ? (T)((double)S.meteo_rate * (double)R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
-                         : (T)S.meteoi;
+        // the melt depth the hydrodynamic step added (FP32 state: melt32 in fx_hydro.cu)
+        T mi;
+        if constexpr (sizeof(T) == 4)
+          mi = Fields<T>::mm(d) ? (T)(S.meteoi * (double)R.mm[slot][lane]) : (T)S.meteoi;
+        else
+          mi = Fields<T>::mm(d) ? (T)((double)S.meteo_rate * (double)R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
+                                : (T)S.meteoi;
         c = tdiv(c * hp + (mi * (T)S.mconc), hm);
       }
     }

@@ -588,6 +588,33 @@ __device__ __forceinline__ float fcbrt(float h) {
   return r;
 }
 
+// The melt depth the FP32 state adds to a cell this step: the step's
+// uniform depth c.meteoi (rate / (1000*3600*24) * dt, computed once in
+// k_finalize) times the cell's melt multiplier, rounded once to float. The
+// budget counts this float value, the water actually added.
+__device__ __forceinline__ float melt32(const fx_dev& d, const StepCtl& c, float mm) {
+  return d.melt_mult_f ? (float)(c.meteoi * (double)mm) : (float)c.meteoi;
+}
+
+// The Courant candidate of main.cpp:300-323 for the FP32 state. It stays
+// FP64, so the FP32 state's dt sequence follows the reference's formula to
+// the last bits, but with two divisions instead of four: depth > hdry, so
+// the reference's max(h, hdry) is h; u0 and v0 share one reciprocal; and
+// min(cfl dxy / (u0 + c0), cfl dxy / (v0 + c0)) = cfl dxy / (max(u0, v0) + c0).
+__device__ __forceinline__ void courant_cell32(const fx_dev& d, double depth, float qx, float qy, double& dtc,
+                                               double& hm) {
+  dtc = __longlong_as_double(0x7ff0000000000000LL);
+  hm = 0.0;
+  if (depth > d.hdry) {
+    const double rh = 1.0 / depth;
+    const double c0 = sqrt(d.gaccl * depth);
+    const double u0 = fmax(.000001, fabs((double)qx * rh)), v0 = fmax(.000001, fabs((double)qy * rh));
+    const double cc = d.cfl_dxy / (fmax(u0, v0) + c0);
+    if (cc == cc) dtc = cc;
+    hm = depth;
+  }
+}
+
 __device__ __forceinline__ float div_dxy_f(const fx_dev& d, float x) {
   return d.dxy_pow2 ? x * (float)d.inv_dxy : fdiv(x, (float)d.dxy);
 }
@@ -849,10 +876,10 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       float h1 = hpre;
       double depth = fx_dd_val(etapre, lo1);
       if (melt_on && !(fl & FX_F_NODATA)) {
-        const double mi = melt_depth(d, c, gi);
-        bmelt = mi * d.arbase;
+        const float mi = melt32(d, c, d.melt_mult_f ? d.melt_mult_f[gi] : 1.0f);
+        bmelt = (double)mi * d.arbase;
         if (d.ade) d.hpm_f[scur + gi] = hpre;
-        fx_dd_add(eta1, lo1, (float)mi);
+        fx_dd_add(eta1, lo1, mi);
         h1 = fmaxf(eta1, 0.0f);
         depth = fx_dd_val(eta1, lo1);
         if (depth <= d.hdry) ld = 0;
@@ -878,7 +905,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         d.fe1_f[scur + gi] = d.fe1_f[sprev + gi];
         d.fn1_f[scur + gi] = d.fn1_f[sprev + gi];
       }
-      courant_cell(d, fmax(0.0, depth), (double)qx, (double)qy, dtc, hm);
+      courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
     }
     reduce_courant(d, S, dtc, hm);
     reduce_budget(d, S.budget, bmelt, 0.0);
@@ -910,9 +937,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         cl = C_INT;
         const uint8_t fl = g_fl[scc * STG_W1 + sr + so.o1];
         if (fl & FX_F_WALL) cl |= C_WALL;
-        if (melt_on && !(fl & FX_F_NODATA))
-          fx_dd_add(eta, lo, (float)(d.melt_mult_f ? (double)c.meteo_rate * (double)g_mm[i4] / (1000. * 3600. * 24.) * c.dtfl
-                                                   : c.meteoi));
+        if (melt_on && !(fl & FX_F_NODATA)) fx_dd_add(eta, lo, melt32(d, c, g_mm[i4]));
         if (is_inflow(d, r, q)) inflow_eta(eta, lo, c.inflowi);
         if (fx_dd_val(eta, lo) <= d.hdry) {
           qx = 0.f;
@@ -945,7 +970,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         cl = C_INT;
         const uint8_t fl = d.flags[sprev + gi];
         if (fl & FX_F_WALL) cl |= C_WALL;
-        if (melt_on && !(fl & FX_F_NODATA)) fx_dd_add(eta, lo, (float)melt_depth(d, c, gi));
+        if (melt_on && !(fl & FX_F_NODATA)) fx_dd_add(eta, lo, melt32(d, c, d.melt_mult_f ? d.melt_mult_f[gi] : 1.0f));
         if (is_inflow(d, r, q)) inflow_eta(eta, lo, c.inflowi);
         if (fx_dd_val(eta, lo) <= d.hdry) {
           qx = 0.f;
@@ -1022,9 +1047,9 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     if (melt_on && !(fl & FX_F_NODATA)) {
       h0v = fmaxf(eta1, 0.0f);
       if (d.ade) d.hpm_f[scur + gi] = fmaxf(etapre, 0.0f);
-      mi = (stg && d.melt_mult_f) ? (double)c.meteo_rate * (double)reinterpret_cast<const float*>(stg + L::O_MM)[i4] /
-                                        (1000. * 3600. * 24.) * c.dtfl
-                                  : melt_depth(d, c, gi);
+      const float mm = !d.melt_mult_f ? 1.0f
+                       : (stg ? reinterpret_cast<const float*>(stg + L::O_MM)[i4] : d.melt_mult_f[gi]);
+      mi = (double)melt32(d, c, mm);
       bmelt = mi * d.arbase;
     }
     if (is_inflow(d, irow, icol)) {  // common.cpp:300-315 (h0 = the depth after the inflow)
@@ -1099,7 +1124,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       d.fe1_f[scur + gi] = 0.0f;
       d.fn1_f[scur + gi] = 0.0f;
     }
-    courant_cell(d, fmax(0.0, depth), (double)qx, (double)qy, dtc, hm);
+    courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
   }
   reduce_courant(d, S, dtc, hm);
   reduce_budget(d, S.budget, bmelt, bout);
@@ -1646,8 +1671,8 @@ __global__ void __launch_bounds__(BX * BY) k_courant_scan(const fx_dev* __restri
     const long long gi = fx_ix(d, irow, icol);
     const long long sl = fx_slot(d, d.ctl->steps), pl = fx_pp(d, d.ctl->steps);
     if (d.prec32)
-      courant_cell(d, fmax(0.0, fx_dd_val(d.eta[pl + gi], d.eta_lo[pl + gi])), (double)d.qx_f[pl + gi],
-                   (double)d.qy_f[pl + gi], dtc, hm);
+      courant_cell32(d, fmax(0.0, fx_dd_val(d.eta[pl + gi], d.eta_lo[pl + gi])), d.qx_f[pl + gi],
+                     d.qy_f[pl + gi], dtc, hm);
     else
       courant_cell(d, d.h[sl + gi], d.qx[pl + gi], d.qy[pl + gi], dtc, hm);
   }
