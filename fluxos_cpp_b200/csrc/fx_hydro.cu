@@ -401,7 +401,9 @@ __device__ __forceinline__ void courant_cell(const fx_dev& d, double h, double q
     double c0 = sqrt(d.gaccl * h);
     double u0 = fmax(.000001, fabs(qx / hp));
     double v0 = fmax(.000001, fabs(qy / hp));
-    double c = fmin(d.cfl_dxy / (u0 + c0), d.cfl_dxy / (v0 + c0));
+    // min(a / (u0 + c0), a / (v0 + c0)) with a > 0 is a / (max(u0, v0) + c0)
+    // bit for bit: rounded addition and division are monotone
+    double c = d.cfl_dxy / (fmax(u0, v0) + c0);
     if (c == c) dtc = c;
     hm = h;
   }
@@ -471,6 +473,7 @@ __device__ __forceinline__ StageOff stage_off(int bx) {
 // The fields of the control block a step kernel reads.
 struct StepCtl {
   double dtfl, meteoi, meteo_rate, mconc, inflowi;
+  double twet_inc;  // dtfl / 3600, the wet-time increment (hydrodynamics_calc.cpp:69-70), once per tile
   long long steps;
   int live, active;
 };
@@ -1060,7 +1063,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       bmelt += (fx_dd_val(eta1, S.eta_lo[sP]) - dm) * d.arbase;
       h0v = fmaxf(eta1, 0.0f);
     }
-    if (!(cl & C_DRY)) d.twet_f[gi] += (float)(c.dtfl / 3600);
+    if (!(cl & C_DRY)) d.twet_f[gi] += (float)c.twet_inc;
     float dh = 0.f, dqx = 0.f, dqy = 0.f, qxfP = 0.f, qyfP = 0.f;
     if (!wall) {
       dh = (div_dxy_f(d, S.f[0][fW] - S.f[0][fP]) + div_dxy_f(d, S.f[3][fS] - S.f[3][fP])) * dtl;
@@ -1359,7 +1362,7 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       h0v = fmax(z1 - zb, 0.0);
     }
     // Loop 1 wet time (:69-70)
-    if (!(cl & C_DRY)) d.twet[gi] += dtl / 3600;
+    if (!(cl & C_DRY)) d.twet[gi] += c.twet_inc;  // dtl / 3600
 
     // Loop 3 (:93-120)
     double dh = 0.0, dqx = 0.0, dqy = 0.0, qxfP = 0.0, qyfP = 0.0;
@@ -1458,6 +1461,7 @@ __device__ __forceinline__ void hydro_block(const fx_dev& d, const fx_tile& tile
     sc.meteo_rate = g.meteo_rate;
     sc.mconc = g.mconc;
     sc.inflowi = g.inflowi;
+    sc.twet_inc = g.dtfl / 3600;
     sc.steps = g.steps;
     sc.live = g.live;
     sc.active = g.active;
@@ -1593,6 +1597,7 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
     sc.meteo_rate = g.meteo_rate;
     sc.mconc = g.mconc;
     sc.inflowi = g.inflowi;
+    sc.twet_inc = g.dtfl / 3600;
     sc.steps = g.steps;
     sc.live = g.live;
     sc.active = g.active;
