@@ -470,6 +470,25 @@ __device__ __forceinline__ StageOff stage_off(int bx) {
   return StageOff{x & 3, x & 1, x & 15};
 }
 
+// A thread's share of a launch's reductions, kept across the tiles it works
+// on and reduced once per block (reduce_part): the smallest Courant dt and
+// the largest wet depth (exact in any order) and the FP64 water budget.
+struct TilePart {
+  double dtc, hm, melt, out;
+  __device__ __forceinline__ void add(double dt, double h, double m, double o) {
+    dtc = fmin(dtc, dt);
+    hm = fmax(hm, h);
+    melt += m;
+    out += o;
+  }
+};
+__device__ __forceinline__ TilePart tile_part() {
+  TilePart p;
+  p.dtc = __longlong_as_double(0x7ff0000000000000LL);
+  p.hm = p.melt = p.out = 0.0;
+  return p;
+}
+
 // The fields of the control block a step kernel reads.
 struct StepCtl {
   double dtfl, meteoi, meteo_rate, mconc, inflowi;
@@ -501,6 +520,14 @@ __device__ void reduce_budget(const fx_dev& d, double* red, double melt, double 
     if (a != 0.0) atomicAdd(&d.ctl->budget_melt, a);
     if (b != 0.0) atomicAdd(&d.ctl->budget_out, b);
   }
+}
+
+// The block's reductions of a launch: Courant dt and wet depth, then the
+// budget (every thread of the block calls it).
+template <class SM>
+__device__ __forceinline__ void reduce_part(const fx_dev& d, SM& S, const TilePart& acc) {
+  reduce_courant(d, S, acc.dtc, acc.hm);
+  reduce_budget(d, S.budget, acc.melt, acc.out);
 }
 
 __device__ __forceinline__ double melt_depth(const fx_dev& d, const StepCtl& c, long long gi) {
@@ -852,7 +879,7 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
 
 template <int BY>
 __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
-                                             HydroSmem32<BY>& S, const unsigned char* stg = nullptr) {
+                                             HydroSmem32<BY>& S, TilePart& acc, const unsigned char* stg = nullptr) {
   using L = StageLayout<true, BY>;
   const StageOff so = stage_off(tile.bx);
   constexpr int TY = Tile<BY>::TY, NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX;
@@ -910,8 +937,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       }
       courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
     }
-    reduce_courant(d, S, dtc, hm);
-    reduce_budget(d, S.budget, bmelt, 0.0);
+    acc.add(dtc, hm, bmelt, 0.0);
     return;
   }
 
@@ -1129,14 +1155,13 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     }
     courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
   }
-  reduce_courant(d, S, dtc, hm);
-  reduce_budget(d, S.budget, bmelt, bout);
+  acc.add(dtc, hm, bmelt, bout);
 }
 
 // The FP64 step of one tile (the reference's arithmetic, bit for bit).
 template <int BY>
 __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
-                                             HydroSmem<BY>& S, const unsigned char* stg = nullptr) {
+                                             HydroSmem<BY>& S, TilePart& acc, const unsigned char* stg = nullptr) {
   using L = StageLayout<false, BY>;
   const StageOff so = stage_off(tile.bx);
   constexpr int TY = Tile<BY>::TY, NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX;
@@ -1197,8 +1222,7 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       }
       courant_cell(d, h1, qx, qy, dtc, hm);
     }
-    reduce_courant(d, S, dtc, hm);
-    reduce_budget(d, S.budget, bmelt, 0.0);
+    acc.add(dtc, hm, bmelt, 0.0);
     return;
   }
 
@@ -1444,8 +1468,7 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     }
     courant_cell(d, h, qx, qy, dtc, hm);
   }
-  reduce_courant(d, S, dtc, hm);
-  reduce_budget(d, S.budget, bmelt, bout);
+  acc.add(dtc, hm, bmelt, bout);
 }
 
 // Reads the step's fields of the control block (written by k_finalize) into
@@ -1469,8 +1492,10 @@ __device__ __forceinline__ void hydro_block(const fx_dev& d, const fx_tile& tile
   __syncthreads();
   const StepCtl c = sc;
   if (!c.live) return;
-  if constexpr (P32) hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S));
-  else hydro_tile64<BY>(d, c, tile, S);
+  TilePart acc = tile_part();
+  if constexpr (P32) hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S), acc);
+  else hydro_tile64<BY>(d, c, tile, S, acc);
+  reduce_part(d, S, acc);
 }
 
 // Blocks per SM the launch bounds ask for: 768 threads for FP64 (at most 85
@@ -1606,13 +1631,15 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
   __syncthreads();
   const StepCtl c = sc;
   if (!c.live) return;
+  TilePart acc = tile_part();
   if (!c.active) {  // no solver this step: cell-local work only, nothing to stage
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
       const fx_tile tile{0, t % ntx, t / ntx, 0};
-      if constexpr (P32) hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S));
-      else hydro_tile64<BY>(d, c, tile, S);
+      if constexpr (P32) hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S), acc);
+      else hydro_tile64<BY>(d, c, tile, S, acc);
       __syncthreads();
     }
+    reduce_part(d, S, acc);
     return;
   }
   if (tid == 0) {
@@ -1651,11 +1678,12 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
     }
     const fx_tile tile{0, t % ntx, t / ntx, 0};
     if constexpr (P32)
-      hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S), stage0 + st * L::BYTES);
-    else hydro_tile64<BY>(d, c, tile, S, stage0 + st * L::BYTES);
+      hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S), acc, stage0 + st * L::BYTES);
+    else hydro_tile64<BY>(d, c, tile, S, acc, stage0 + st * L::BYTES);
     __syncthreads();  // the stage is free for the load issued two tiles later
     st ^= 1;
   }
+  reduce_part(d, S, acc);
 }
 
 // Courant scan of the state as uploaded (the scan at the top of the first
