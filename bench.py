@@ -99,9 +99,19 @@ class ClockSampler:
         self.proc = None
         self.path = None
 
+    def _lines(self) -> int:
+        try:
+            with open(self.path) as f:
+                return sum(1 for ln in f if ln.count(",") >= 7)
+        except Exception:
+            return 0
+
     def start(self):
+        """Start sampling and return once samples are flowing (nvidia-smi
+        takes a moment to start); samples before this point are not kept."""
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
+        self.n0 = 0
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
@@ -109,11 +119,21 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        time.sleep(0.15)
+            return
+        t0 = time.time()
+        while self._lines() == 0 and time.time() - t0 < 10.0:
+            time.sleep(0.02)
+        self.n0 = self._lines()
 
     def stop(self) -> dict:
+        """Stop after one more sample than there was at the end of the timed
+        region (so a short region still has one); keep the samples taken
+        since start() returned."""
         if self.proc is not None:
-            time.sleep(0.06)
+            n1 = self._lines()
+            t0 = time.time()
+            while self._lines() <= n1 and time.time() - t0 < 1.0:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -128,6 +148,7 @@ class ClockSampler:
             os.unlink(self.path)
         except Exception:
             pass
+        rows = rows[getattr(self, "n0", 0):]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         sm = [float(r[0]) for r in rows if r[0].replace(".", "", 1).isdigit()]
