@@ -323,6 +323,8 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
     for (float** f : slot_fields)
       if ((rc = dev_alloc(c, (void**)f, pf * d.nslot)) != FX_OK) goto fail;
     if ((rc = dev_alloc(c, (void**)&d.conc_f, pf * g->nchem)) != FX_OK) goto fail;
+    if ((rc = dev_alloc(c, (void**)&c->stage, (size_t)d.plane * sizeof(double))) != FX_OK) goto fail;
+    if ((rc = dev_alloc(c, (void**)&c->zstage, (size_t)d.plane * sizeof(double))) != FX_OK) goto fail;
   }
   if (d.wintra && (rc = alloc_soil(c)) != FX_OK) goto fail;
   if ((rc = dev_alloc(c, (void**)&c->d_mass, sizeof(double) * (1 + FX_MAX_CHEM))) != FX_OK) goto fail;
@@ -420,8 +422,8 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
   const long long strips = (g->nrows + fx_ade_rows_per_strip() - 1) / fx_ade_rows_per_strip();
   const long long gx = (g->nrows + 30) / 31, gy = (g->ncols + 6) / 7;
   long long b = 0;
-  if (p->precision == 1)
-    b += plane * (8 + 5 * 4 + 4 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids);
+  if (p->precision == 1)  // zb, twet and the flux fields, pairs, slots, solutes, extensions, 2 staging planes
+    b += plane * (8 + 5 * 4 + 4 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids + 16);
   else
     b += plane * (6 * 8 + 3 * 2 * 8 + 5 * 8 * nslot + 8LL * g->nchem + 8LL * extension_grids);
   if (p->wintra && p->ade) b += plane * g->nchem * (p->precision == 1 ? 4 : 8);  // soil mass
@@ -436,70 +438,106 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
 
 // Copies a host grid (double, GlobVar layout) into `planes` consecutive
 // planes of a device field, converting to float for FP32 fields.
-static int put_grid(fx_ctx* c, void* dst, bool f32, int planes, const double* host) {
+// Elementwise conversions over whole planes in the field layout (the
+// padding rows are 0 on both sides and stay 0).
+__global__ void k_f64_to_f32(const double* __restrict__ src, float* __restrict__ dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+__global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__ dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+// z = zb + (eta + eta_lo) of the FP32 state (the order of get_z32's host sum before).
+__global__ void k_z_of_eta(const double* __restrict__ zb, const float* __restrict__ eta,
+                           const float* __restrict__ lo, double* __restrict__ z, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    z[i] = zb[i] + ((double)eta[i] + (double)lo[i]);
+}
+static int plane_grid(long long n) { return (int)std::min<long long>((n + 255) / 256, 148 * 16); }
+
+// Host grid (FP64, GlobVar layout) -> device plane in the field layout: one
+// pitched copy, straight into an FP64 field, or into the staging plane and
+// converted on the device for an FP32 field.
+static int copy_in(fx_ctx* c, double* dst64, const double* host) {
   const int mr = c->d.nr + 2, mc = c->d.nc + 2;
-  const size_t esz = f32 ? sizeof(float) : sizeof(double);
-  std::vector<float> tmp;
-  const void* src = host;
-  if (f32) {
-    tmp.resize((size_t)mr * mc);
-    for (size_t i = 0; i < tmp.size(); ++i) tmp[i] = (float)host[i];
-    src = tmp.data();
+  FX_CK(c, cudaMemcpy2DAsync(dst64 + FX_ROFF, (size_t)c->d.ld * sizeof(double), host, (size_t)mr * sizeof(double),
+                             (size_t)mr * sizeof(double), (size_t)mc, cudaMemcpyHostToDevice, c->stream));
+  return FX_OK;
+}
+static int copy_out(fx_ctx* c, double* host, const double* src64) {
+  const int mr = c->d.nr + 2, mc = c->d.nc + 2;
+  FX_CK(c, cudaMemcpy2DAsync(host, (size_t)mr * sizeof(double), src64 + FX_ROFF, (size_t)c->d.ld * sizeof(double),
+                             (size_t)mr * sizeof(double), (size_t)mc, cudaMemcpyDeviceToHost, c->stream));
+  return FX_OK;
+}
+
+static int put_grid(fx_ctx* c, void* dst, bool f32, int planes, const double* host) {
+  int rc;
+  if (!f32) {
+    for (int k = 0; k < planes; ++k)
+      if ((rc = copy_in(c, (double*)dst + k * c->d.plane, host))) return rc;
+  } else {
+    if ((rc = copy_in(c, c->stage, host))) return rc;
+    for (int k = 0; k < planes; ++k)
+      k_f64_to_f32<<<plane_grid(c->d.plane), 256, 0, c->stream>>>(c->stage, (float*)dst + k * c->d.plane,
+                                                                   c->d.plane);
+    FX_CK(c, cudaGetLastError());
   }
-  for (int k = 0; k < planes; ++k)
-    FX_CK(c, cudaMemcpy2DAsync((char*)dst + (k * c->d.plane + FX_ROFF) * esz, (size_t)c->d.ld * esz, src,
-                               (size_t)mr * esz, (size_t)mr * esz, (size_t)mc, cudaMemcpyHostToDevice, c->stream));
   FX_CK(c, cudaStreamSynchronize(c->stream));
   return FX_OK;
 }
 
 // Copies one plane of a device field into a host grid (double).
 static int get_grid(fx_ctx* c, const void* src, bool f32, double* host) {
-  const int mr = c->d.nr + 2, mc = c->d.nc + 2;
-  const size_t esz = f32 ? sizeof(float) : sizeof(double);
-  std::vector<float> tmp;
-  void* dst = host;
-  if (f32) {
-    tmp.resize((size_t)mr * mc);
-    dst = tmp.data();
+  int rc;
+  if (!f32) {
+    rc = copy_out(c, host, (const double*)src);
+  } else {
+    k_f32_to_f64<<<plane_grid(c->d.plane), 256, 0, c->stream>>>((const float*)src, c->stage, c->d.plane);
+    FX_CK(c, cudaGetLastError());
+    rc = copy_out(c, host, c->stage);
   }
-  FX_CK(c, cudaMemcpy2DAsync(dst, (size_t)mr * esz, (const char*)src + FX_ROFF * esz, (size_t)c->d.ld * esz,
-                             (size_t)mr * esz, (size_t)mc, cudaMemcpyDeviceToHost, c->stream));
+  if (rc) return rc;
   FX_CK(c, cudaStreamSynchronize(c->stream));
-  if (f32)
-    for (size_t i = 0; i < tmp.size(); ++i) host[i] = (double)tmp[i];
   return FX_OK;
 }
 
-// FP32 state: z = zb + eta on the host (or the z still waiting for fx_prepare).
-static int get_z32(fx_ctx* c, double* host) {
-  const size_t n = (size_t)(c->d.nr + 2) * (c->d.nc + 2);
-  if (!c->z_pending.empty()) {
-    std::copy(c->z_pending.begin(), c->z_pending.end(), host);
-    return FX_OK;
-  }
-  std::vector<double> eta(n), lo(n);
+// FP32 state: the current z = zb + (eta + eta_lo) into the device plane `z`
+// (field layout).
+static int z32_into(fx_ctx* c, double* z) {
   int rc = read_ctl(c);
-  if (!rc) rc = get_grid(c, c->d.zb, false, host);
-  if (!rc) rc = get_grid(c, c->d.eta + fx_pp(c->d, c->ctl_host->steps), true, eta.data());
-  if (!rc) rc = get_grid(c, c->d.eta_lo + fx_pp(c->d, c->ctl_host->steps), true, lo.data());
   if (rc) return rc;
-  for (size_t i = 0; i < n; ++i) host[i] += eta[i] + lo[i];
+  const long long pp = fx_pp(c->d, c->ctl_host->steps);
+  k_z_of_eta<<<plane_grid(c->d.plane), 256, 0, c->stream>>>(c->d.zb, c->d.eta + pp, c->d.eta_lo + pp, z,
+                                                            c->d.plane);
+  FX_CK(c, cudaGetLastError());
+  return FX_OK;
+}
+
+// FP32 state: z on the host (the z still waiting for fx_prepare, if any).
+static int get_z32(fx_ctx* c, double* host) {
+  int rc;
+  if (!c->z_pending && (rc = z32_into(c, c->stage))) return rc;
+  if ((rc = copy_out(c, host, c->z_pending ? c->zstage : c->stage))) return rc;
+  FX_CK(c, cudaStreamSynchronize(c->stream));
   return FX_OK;
 }
 
 int fx_upload(fx_ctx* c, const char* field, const double* host) {
   if (!c || !field || !host) return fx_fail(c, FX_ERR_ARG, "fx_upload: null argument");
   if (!known_field(c, field)) return fx_fail(c, FX_ERR_ARG, "fx_upload: unknown field '%s'", field);
-  const size_t n = (size_t)(c->d.nr + 2) * (c->d.nc + 2);
   int rc;
   if (c->d.prec32 && !strcmp(field, "z")) {
-    c->z_pending.assign(host, host + n);  // converted by fx_prepare with the bed then current
+    // converted by fx_prepare with the bed then current
+    if ((rc = copy_in(c, c->zstage, host))) return rc;
+    FX_CK(c, cudaStreamSynchronize(c->stream));
+    c->z_pending = true;
   } else if (c->d.prec32 && !strcmp(field, "zb")) {
     // z stays what it was (as for FP64 state): keep it until fx_prepare
-    if (c->z_pending.empty()) {
-      c->z_pending.resize(n);
-      if ((rc = get_z32(c, c->z_pending.data()))) return rc;
+    if (!c->z_pending) {
+      if ((rc = z32_into(c, c->zstage))) return rc;
+      c->z_pending = true;
     }
     if ((rc = put_grid(c, c->d.zb, false, 1, host))) return rc;
   } else {
@@ -554,9 +592,12 @@ int fx_upload_flags(fx_ctx* c, const float* ldry, const float* wall) {
   std::vector<uint8_t> fl((size_t)mr * mc);
   for (size_t i = 0; i < fl.size(); ++i)
     fl[i] = (uint8_t)((ldry[i] == 1.0f ? FX_F_LDRY : 0) | (wall[i] == 1.0f ? FX_F_WALL : 0));
-  for (int k = 0; k < c->d.nslot; ++k)
-    FX_CK(c, cudaMemcpy2DAsync(c->d.flags + k * c->d.plane + FX_ROFF, (size_t)c->d.ld, fl.data(), (size_t)mr,
-                               (size_t)mr, (size_t)mc, cudaMemcpyHostToDevice, c->stream));
+  // one copy from the host, then device-to-device into the other slot planes
+  FX_CK(c, cudaMemcpy2DAsync(c->d.flags + FX_ROFF, (size_t)c->d.ld, fl.data(), (size_t)mr, (size_t)mr, (size_t)mc,
+                             cudaMemcpyHostToDevice, c->stream));
+  for (int k = 1; k < c->d.nslot; ++k)
+    FX_CK(c, cudaMemcpyAsync(c->d.flags + k * c->d.plane, c->d.flags, (size_t)c->d.plane, cudaMemcpyDeviceToDevice,
+                             c->stream));
   FX_CK(c, cudaStreamSynchronize(c->stream));
   c->prepared = false;
   return FX_OK;
@@ -708,26 +749,12 @@ int fx_prepare(fx_ctx* c) {
   FX_CK(c, cudaMemcpyAsync(c->d.ctl, c->ctl_host, sizeof(fx_ctl), cudaMemcpyHostToDevice, c->stream));
   if ((rc = fx_sync_dev(c))) return rc;
   if (c->d.prec32) {
-    if (!c->z_pending.empty()) {
-      // stage z in the field layout and convert it with the current bed
-      double* z = nullptr;
-      FX_CK(c, cudaMalloc((void**)&z, (size_t)c->d.plane * sizeof(double)));
-      int r2 = FX_OK;
-      const int mr = c->d.nr + 2, mc = c->d.nc + 2;
-      cudaError_t e = cudaMemsetAsync(z, 0, (size_t)c->d.plane * sizeof(double), c->stream);
-      if (e == cudaSuccess)
-        e = cudaMemcpy2DAsync(z + FX_ROFF, (size_t)c->d.ld * sizeof(double), c->z_pending.data(),
-                              (size_t)mr * sizeof(double), (size_t)mr * sizeof(double), (size_t)mc,
-                              cudaMemcpyHostToDevice, c->stream);
-      if (e == cudaSuccess) {
-        fx_launch_eta_from_z(c->d, z, c->stream);
-        e = cudaGetLastError();
-      }
-      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-      if (e != cudaSuccess) r2 = fx_fail(c, FX_ERR_CUDA, "FP32 depth conversion failed: %s", cudaGetErrorString(e));
-      cudaFree(z);
-      if (r2) return r2;
-      c->z_pending.clear();
+    if (c->z_pending) {
+      // the pending z (field layout) with the current bed
+      fx_launch_eta_from_z(c->d, c->zstage, c->stream);
+      FX_CK(c, cudaGetLastError());
+      FX_CK(c, cudaStreamSynchronize(c->stream));
+      c->z_pending = false;
     }
   }
   fx_launch_mark_static(c->d_dev, 0, c->stream);

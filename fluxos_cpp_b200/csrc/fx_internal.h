@@ -32,10 +32,14 @@ struct fx_ctx {
   bool store_all_opt = false;
   bool negative_forcing = false;
   cudaGraphExec_t graph_exec = nullptr;
-  // FP32 state: z is held as eta = z - zb. An uploaded z (or the z of the
-  // state when zb is replaced) waits here until fx_prepare converts it with
-  // the bed then on the device.
-  std::vector<double> z_pending;
+  // FP32 state: host grids (FP64) cross to and from the device through
+  // `stage`, one FP64 plane in the field layout, and are converted there by
+  // kernels; z is held as eta = z - zb, so an uploaded z (or the z of the
+  // state when zb is replaced) waits in `zstage` until fx_prepare converts
+  // it with the bed then current (`z_pending`).
+  double* stage = nullptr;
+  double* zstage = nullptr;
+  bool z_pending = false;
   double* d_mass = nullptr;    // fx_mass result: water, then one mass per solute
   // TMA-staged hydrodynamic kernel (one domain): tensor maps of the stencil
   // fields, rebuilt with the descriptor; its persistent grid size

@@ -1023,7 +1023,7 @@ int fx_write_results_host(const char* path, int nrows, int ncols, int dxy, doubl
 int fx_write_results_async(fx_ctx* c, const char* path) {
   if (!c) return FX_ERR_ARG;
   int rc;
-  if (c->d.prec32 && !c->z_pending.empty() && (rc = fx_prepare(c))) return rc;
+  if (c->d.prec32 && c->z_pending && (rc = fx_prepare(c))) return rc;
   fx_status st;
   if ((rc = fx_get_status(c, &st))) return rc;
   std::string fn;
