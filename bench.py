@@ -78,6 +78,24 @@ def _rank():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def max_over_ranks(x: float, device: str = "cuda") -> float:
+    """The largest of every rank's x (a job is as slow as its slowest
+    replica), or x itself without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, world: int, seconds: float) -> float:
+    """Whole-job throughput of `world` replicas that each processed
+    `units_per_rank` units, timed as the slowest rank's `seconds`."""
+    return units_per_rank * world / seconds
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -522,19 +540,18 @@ def run_gpu(args):
         res[p] = measure_domain(doms[p], args.steps, args.warmup, cells, p, peak, gpu, args.tile_rows)
     torch.cuda.synchronize()
     head = precs[0]
-    t = torch.tensor([res[head]["ms_total"]], dtype=torch.float64, device="cuda")
+    ms_max = max_over_ranks(res[head]["ms_total"])
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    ms_max = float(t.item())
-    value = cells * args.steps * world / (ms_max / 1e3)
+    value = job_rate(cells * args.steps, world, ms_max / 1e3)
     acc = None
     if len(precs) == 2:
         acc = accuracy_of(doms["fp32"], doms["fp64"], w0["fp32"], w0["fp64"], sc.ks)
     e2e = None
     if not args.no_e2e:
         secs, h2d, d2h, parts = e2e_run(doms[head], sc, args.steps, k_batch)
-        e2e = {"value": cells * args.steps / secs, "unit": "cell-updates/s", "parts": parts,
+        secs = max_over_ranks(secs)
+        e2e = {"value": job_rate(cells * args.steps, world, secs), "unit": "cell-updates/s", "parts": parts,
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                "note": "upload of the state from pinned host memory, the K steps through fx_step in "
                        "calls of steps-in-flight steps (each call reads the control block with every "
