@@ -580,6 +580,9 @@ struct HydroSmem32 {
   double red_dt[NW], red_h[NW];
   double zb[NSTEN];
   float eta[NSTEN], eta_lo[NSTEN], qx[NSTEN], qy[NSTEN];
+  // cell velocities q / max(h, hdry, ks) of the stencil, formed once per
+  // cell for the wet solver's shear terms (each face reads eight of them)
+  float u[NSTEN], v[NSTEN];
   float f[6][NFLUX];
   unsigned char cls[NSTEN];
 };
@@ -729,15 +732,17 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   const float hnn = nueml * fsqrt(hp * hn);
   const float rhp0 = frcp(hp0);
   const float up = qp * rhp0;
-  const float un = fdiv(qn, fmaxf(fmaxf(hn, hdryl), ksat(N)));
-  const float us0 = fdiv(S.qx[Sx], fmaxf(fmaxf(hs, hdryl), ksat(Sx)));
-  const float use0 = fdiv(S.qx[ES], fmaxf(fmaxf(hat(ES), hdryl), ksat(ES)));
-  const float une = fdiv(S.qx[EN], fmaxf(fmaxf(hat(EN), hdryl), ksat(EN)));
+  // neighbour velocities from the stencil (a dry neighbour's discharge is 0,
+  // so its velocity is 0 whatever depth the division uses)
+  const float un = S.u[N];
+  const float us0 = S.u[Sx];
+  const float use0 = S.u[ES];
+  const float une = S.u[EN];
   const float vp = rp * rhp0;
-  const float ve = fdiv(re, fmaxf(fmaxf(he, hdryl), ksat(E)));
-  const float vw = fdiv(rw, fmaxf(fmaxf(hw, hdryl), ksat(W)));
-  const float vwn = fdiv(S.qy[WN], fmaxf(fmaxf(hat(WN), hdryl), ksat(WN)));
-  const float ven = fdiv(S.qy[EN], fmaxf(fmaxf(hat(EN), hdryl), ksat(EN)));
+  const float ve = S.v[E];
+  const float vw = S.v[W];
+  const float vwn = S.v[WN];
+  const float ven = S.v[EN];
   const float txye = hne * (div_dxy_f(d, ve - vp) + div_dxy_f(d, .25f * (un + une - us0 - use0)));
   const float txyn = hnn * (div_dxy_f(d, un - up) + div_dxy_f(d, .25f * (ve + ven - vw - vwn)));
   const float fe1c = qme, fe2c = qme * ume, fe3c = qme * vme - txye;
@@ -973,6 +978,11 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       S.qx[k] = qx;
       S.qy[k] = qy;
       S.cls[k] = cl;
+      {
+        const float den = fmaxf(fmaxf(fmaxf(0.0f, eta), (float)d.hdry), (cl & C_INT) ? (float)d.ks : 0.0f);
+        S.u[k] = fdiv(qx, den);
+        S.v[k] = fdiv(qy, den);
+      }
     }
   } else
   for (int k = tid; k < NSTEN; k += NTHREADS) {
@@ -1007,6 +1017,11 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     S.qx[k] = qx;
     S.qy[k] = qy;
     S.cls[k] = cl;
+      {
+        const float den = fmaxf(fmaxf(fmaxf(0.0f, eta), (float)d.hdry), (cl & C_INT) ? (float)d.ks : 0.0f);
+        S.u[k] = fdiv(qx, den);
+        S.v[k] = fdiv(qy, den);
+      }
   }
   __syncthreads();
   {
