@@ -55,6 +55,12 @@ struct HydroSmem {
   static constexpr int NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX, NW = Tile<BY>::NTHREADS / 32;
   double budget[2 * NW];
   double z[NSTEN], zb[NSTEN], qx[NSTEN], qy[NSTEN];
+  // cell velocities q / max(h, hdry, ks) of the stencil, formed once per
+  // cell for the wet solver's shear terms (the same expression and operands
+  // the solver divides for each face, so the same values); kept for tiles
+  // up to 8 rows, the largest tile's state stays within 48 KB
+  static constexpr bool VEL = BY <= 8;
+  double u[VEL ? NSTEN : 1], v[VEL ? NSTEN : 1];
   double f[6][NFLUX];
   unsigned char cls[NSTEN];
   short wet_list[NFLUX], dry_list[NFLUX], stale_list[NFLUX];
@@ -208,15 +214,31 @@ __device__ void solver_wet(const fx_dev& d, const SM& S, int sr, int sc, int iro
   const double hnn = .5 * (cnp + cnn) * sqrt(hp * hn);
 
   const double up = qp / hp0;
-  const double un = qn / fmax(fmax(hn, hdryl), ksat(N));
-  const double us0 = S.qx[Sx] / fmax(fmax(hs, hdryl), ksat(Sx));
-  const double use0 = S.qx[ES] / fmax(fmax(hat(ES), hdryl), ksat(ES));
-  const double une = S.qx[EN] / fmax(fmax(hat(EN), hdryl), ksat(EN));
+  // neighbour velocities from the stencil (solver_wetdomain.cpp: each is
+  // q / max(max(h, hdry), ks) of its cell; a dry neighbour's discharge is 0,
+  // so its velocity is 0 whatever depth the division uses)
+  double un, us0, use0, une, ve, vw, vwn, ven;
+  if constexpr (SM::VEL) {
+    un = S.u[N];
+    us0 = S.u[Sx];
+    use0 = S.u[ES];
+    une = S.u[EN];
+    ve = S.v[E];
+    vw = S.v[W];
+    vwn = S.v[WN];
+    ven = S.v[EN];
+  } else {
+    un = qn / fmax(fmax(hn, hdryl), ksat(N));
+    us0 = S.qx[Sx] / fmax(fmax(hs, hdryl), ksat(Sx));
+    use0 = S.qx[ES] / fmax(fmax(hat(ES), hdryl), ksat(ES));
+    une = S.qx[EN] / fmax(fmax(hat(EN), hdryl), ksat(EN));
+    ve = re / fmax(fmax(he, hdryl), ksat(E));
+    vw = rw / fmax(fmax(hw, hdryl), ksat(W));
+    vwn = S.qy[WN] / fmax(fmax(hat(WN), hdryl), ksat(WN));
+    ven = S.qy[EN] / fmax(fmax(hat(EN), hdryl), ksat(EN));
+  }
   const double vp = rp / hp0;
-  const double ve = re / fmax(fmax(he, hdryl), ksat(E));
-  const double vw = rw / fmax(fmax(hw, hdryl), ksat(W));
-  const double vwn = S.qy[WN] / fmax(fmax(hat(WN), hdryl), ksat(WN));
-  const double ven = S.qy[EN] / fmax(fmax(hat(EN), hdryl), ksat(EN));
+
 
   const double txye = hne * (fx_div_dxy(d, ve - vp) + fx_div_dxy(d, .25 * (un + une - us0 - use0)));
   const double txyn = hnn * (fx_div_dxy(d, un - up) + fx_div_dxy(d, .25 * (ve + ven - vw - vwn)));
@@ -582,6 +604,7 @@ struct HydroSmem32 {
   float eta[NSTEN], eta_lo[NSTEN], qx[NSTEN], qy[NSTEN];
   // cell velocities q / max(h, hdry, ks) of the stencil, formed once per
   // cell for the wet solver's shear terms (each face reads eight of them)
+  static constexpr bool VEL = true;
   float u[NSTEN], v[NSTEN];
   float f[6][NFLUX];
   unsigned char cls[NSTEN];
@@ -1261,6 +1284,11 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       S.qx[k] = qx;
       S.qy[k] = qy;
       S.cls[k] = cl;
+      if constexpr (HydroSmem<BY>::VEL) {
+        const double den = fmax(fmax(fmax(0.0, z - zb), d.hdry), (cl & C_INT) ? d.ks : 0.0);
+        S.u[k] = qx / den;
+        S.v[k] = qy / den;
+      }
     }
   } else
   for (int k = tid; k < NSTEN; k += NTHREADS) {
@@ -1292,6 +1320,11 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     S.qx[k] = qx;
     S.qy[k] = qy;
     S.cls[k] = cl;
+    if constexpr (HydroSmem<BY>::VEL) {
+      const double den = fmax(fmax(fmax(0.0, z - zb), d.hdry), (cl & C_INT) ? d.ks : 0.0);
+      S.u[k] = qx / den;
+      S.v[k] = qy / den;
+    }
   }
   __syncthreads();
 
