@@ -69,8 +69,8 @@ ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
 # case of this workload, one launch, divided by the cells and the steps the
 # launch covers); traffic scales with the cells, so `traffic` in the line is
 # this times the cells of the run.
-DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 149.35, "k_ade_sweep": 61.35},
-                       "fp32": {"k_hydro": 80.78, "k_ade_sweep": 26.65}}
+DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 143.59, "k_ade_sweep": 61.35},
+                       "fp32": {"k_hydro": 80.38, "k_ade_sweep": 26.65}}
 
 
 def _rank():
