@@ -98,6 +98,22 @@ def case_wintra() -> dict:
     return dict(sc=sc, wet=_patch(24, 20, 5), soil=soil, steps=(1, 10, 100, 400), mode=0, results=False)
 
 
+def case_inflow_wintra() -> dict:
+    """Point inflow, melt and the WINTRA soil release in the same steps, on a
+    wet patchwork with walls (the inflow's dilution and the soil release
+    both change the inflow cell's concentration)."""
+    sc = S.plane_scenario(24, 20, seed=5)
+    sc.horizon = 3000.0
+    sc.wintra = True
+    sc.soil_release_rate = 1.0
+    sc.inflow = ((0.0, 0.01, 3.0), (100.0, 0.03, 0.5), (250.0, 0.0, 0.0))
+    sc.inflow_xy = (20, 24)  # icol 10, irow 12 at dxy 2
+    sc.dem[3, 5:9] = -9999.0
+    rng = np.random.default_rng(13)
+    soil = rng.uniform(0.0, 30.0, (24, 20))
+    return dict(sc=sc, wet=_patch(24, 20, 7), soil=soil, steps=(1, 10, 100, 400), mode=0, results=False)
+
+
 CASES = {
     "plane_walls": case_plane_walls,
     "patchwork_weir": lambda: case_patchwork(0),
@@ -105,6 +121,7 @@ CASES = {
     "dambreak": case_dambreak,
     "inflow": case_inflow,
     "wintra": case_wintra,
+    "inflow_wintra": case_inflow_wintra,
 }
 
 

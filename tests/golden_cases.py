@@ -7,7 +7,7 @@ import numpy as np
 from fluxos_cpp_b200 import scenarios as S
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ("plane_walls", "patchwork_weir", "patchwork_closed", "dambreak", "inflow", "wintra")
+CASES = ("plane_walls", "patchwork_weir", "patchwork_closed", "dambreak", "inflow", "wintra", "inflow_wintra")
 
 
 def load(name: str):
