@@ -2,7 +2,7 @@
 
 Run from the repository root where the reference tree is mounted:
 
-    make -C oracle all && python tests/golden/make_golden.py [case ...]
+    make -C oracle all REF=<FLUXOS_cpp tree> && python tests/golden/make_golden.py [case ...]
 
 Each case is a small seeded scenario. Its input files are written exactly as
 the reference reads them, and the reference sources compiled in
@@ -185,7 +185,7 @@ def build_case(name: str, spec: dict) -> None:
 
 def main() -> None:
     if not P.ref_available(0):
-        sys.exit("oracle/_ref is not built: run `make -C oracle all` with the reference present")
+        sys.exit("oracle/_ref is not built: run `make -C oracle all REF=<FLUXOS_cpp tree>`")
     only = set(sys.argv[1:])
     for name, fn in CASES.items():
         if not only or name in only:
