@@ -17,9 +17,19 @@ launches, each with its own clock and dt:
   between chunks, its result is taken and its memory freed, which makes room
   for the next arrivals.
 
-A request's preparation (input generation, context creation and upload) runs
-on a host thread once it has arrived, while the batch keeps stepping. Latency
-of a request is the time from its arrival to its retirement.
+A request's inputs (terrain, forcing, start state) come with it, as a real
+request's would: a look-ahead generator builds them on host threads before
+the request's arrival time, off the latency clock. Its preparation (context
+creation and upload on the context's own stream) runs on a host thread once
+it has arrived and fits, while the batch keeps stepping. Latency of a
+request is the time from its arrival to its retirement, reported with its
+parts: admission wait (arrival to the start of its preparation),
+preparation, join wait and device residency (joining the batch to
+retirement).
+
+With several GPUs, each rank serves its own share of the request stream
+(`shard`: request id modulo the number of ranks), with its own batch and no
+collective on the data path; `summarize` merges the ranks' records.
 """
 from __future__ import annotations
 
@@ -36,7 +46,7 @@ import fluxos_cpp_b200 as fx
 from fluxos_cpp_b200 import scenarios as S
 
 
-@dataclass
+@dataclass(eq=False)
 class Request:
     """One scenario solve. `make` builds the Scenario (called on a host
     thread); `cells`, `nchem` and `extension_grids` size the admission."""
@@ -51,6 +61,9 @@ class Request:
     precision: str = "fp32"
     steps_in_flight: int = 8
     # filled in by the server
+    inputs: Optional[S.Scenario] = None  # generated ahead of arrival
+    prep_start: Optional[float] = None
+    prepared: Optional[float] = None
     admitted: Optional[float] = None
     done: Optional[float] = None
     steps: int = 0
@@ -70,11 +83,14 @@ class Request:
 class Server:
     """The request loop. `keep` names fields to download at retirement
     (e.g. ("h", "conc")); `on_output(req, domain)` runs for every due output
-    before it is acknowledged."""
+    before it is acknowledged. `batch_factory` and `make_domain` build the
+    batch and a request's domain (fx.Batch and scenarios.make_domain; tests
+    of the host logic pass stand-ins)."""
 
     def __init__(self, cap_bytes: float = 150e9, chunk_steps: int = 32, keep=(),
                  on_output: Optional[Callable] = None, host_threads: int = 4,
-                 clock: Callable[[], float] = time.perf_counter):
+                 clock: Callable[[], float] = time.perf_counter,
+                 batch_factory: Optional[Callable] = None, make_domain: Optional[Callable] = None):
         self.cap = float(cap_bytes)
         self.chunk = int(chunk_steps)
         self.keep = tuple(keep)
@@ -82,7 +98,8 @@ class Server:
         self.clock = clock
         self.pool = cf.ThreadPoolExecutor(max_workers=host_threads)
         self.lookahead = host_threads
-        self.batch = fx.Batch()
+        self.batch = (batch_factory or fx.Batch)()
+        self.make_domain = make_domain or S.make_domain
         self.active: List[tuple] = []  # (request, domain, bytes)
         self.used = 0
         self.peak_used = 0
@@ -114,33 +131,71 @@ class Server:
         self.used -= nbytes
         r.done = now
 
-    def _prepare(self, r: Request):
-        """Host thread: the request's inputs and its resident domain."""
-        sc = r.make()
-        return S.make_domain(sc, precision=r.precision, steps_in_flight=r.steps_in_flight)
+    def _prepare(self, r: Request, t0: float, gen: Optional[cf.Future] = None):
+        """Host thread: the request's resident domain from its inputs (made
+        here only if the look-ahead generator has not made them; `gen` is the
+        generator's unfinished job for them, if any)."""
+        r.prep_start = self.clock() - t0
+        if gen is not None:
+            gen.result()
+        sc = r.inputs if r.inputs is not None else r.make()
+        r.inputs = None
+        d = self.make_domain(sc, precision=r.precision, steps_in_flight=r.steps_in_flight)
+        r.prepared = self.clock() - t0
+        return d
 
-    def run(self, requests: List[Request]) -> dict:
+    def run(self, requests: List[Request], generate_ahead: float = 0.0,
+            generator_threads: int = 4) -> dict:
         """Serve `requests` (arrival times in seconds from the call) to the
-        end; returns throughput and latency figures.
+        end; returns throughput and latency figures (summarize).
 
-        A request's preparation (input generation, device allocation and
-        upload on the request's own stream) starts when it has arrived and
-        its footprint fits under the cap beside the resident members and the
-        preparations in progress; it runs on a host thread while the batch
-        keeps stepping. Prepared requests join the batch between chunks."""
-        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        With generate_ahead > 0, a request's inputs are generated on
+        `generator_threads` host threads from that many seconds before its
+        arrival (off the latency clock; the count of requests whose inputs
+        were not ready at arrival is reported). A request's preparation
+        (device allocation and upload on the request's own stream) starts
+        when it has arrived and its footprint fits under the cap beside the
+        resident members and the preparations in progress; it runs on a host
+        thread while the batch keeps stepping. Prepared requests join the
+        batch between chunks."""
+        order = sorted(requests, key=lambda r: r.arrival)
+        pending = collections.deque(order)
+        to_generate = collections.deque(order if generate_ahead > 0 else [])
+        gen_pool = cf.ThreadPoolExecutor(max_workers=generator_threads) if generate_ahead > 0 else None
+        generating: Dict[int, cf.Future] = {}
+        late_inputs = 0
         preparing = collections.OrderedDict()  # rid -> (request, future, reserved bytes)
         reserved = 0
         t0 = self.clock()
+
+        def _gen(r):
+            r.inputs = r.make()
+
         while pending or preparing or self.active:
             now = self.clock() - t0
+            # the look-ahead generator: inputs of requests arriving within generate_ahead
+            while to_generate and to_generate[0].arrival <= now + generate_ahead and \
+                    len(generating) < 2 * generator_threads:
+                r = to_generate.popleft()
+                generating[r.rid] = gen_pool.submit(_gen, r)
+            for rid in [k for k, f in generating.items() if f.done()]:
+                generating.pop(rid).result()
             # start preparations in arrival order while memory and threads allow
             while pending and pending[0].arrival <= now and len(preparing) < self.lookahead:
                 r = pending[0]
                 need = self.footprint(r)
                 if (self.active or preparing) and self.used + reserved + need > self.cap:
                     break
-                preparing[r.rid] = (r, self.pool.submit(self._prepare, r), need)
+                gen = None
+                if gen_pool is not None:
+                    gen = generating.pop(r.rid, None)
+                    if gen is not None and not gen.done():
+                        late_inputs += 1  # its preparation waits for the generator
+                    elif gen is None and r.inputs is None:
+                        late_inputs += 1  # not started: its preparation makes the inputs
+                        if r in to_generate:
+                            to_generate.remove(r)
+                preparing[r.rid] = (r, self.pool.submit(self._prepare, r, t0, gen), need)
                 reserved += need
                 pending.popleft()
             # admit finished preparations
@@ -177,17 +232,64 @@ class Server:
                 if st["finished"]:
                     self._retire(i, now)
         wall = self.clock() - t0
-        lat = np.array([r.latency for r in requests if r.latency is not None])
-        wait = np.array([r.admitted - r.arrival for r in requests if r.admitted is not None])
-        return {"requests": len(requests), "wall_s": wall,
-                "cell_updates": self.cell_updates,
-                "cell_updates_per_s": self.cell_updates / wall if wall > 0 else 0.0,
-                "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
-                "p99_s": float(np.percentile(lat, 99)) if lat.size else None,
-                "admission_p50_s": float(np.percentile(wait, 50)) if wait.size else None,
-                "admission_p99_s": float(np.percentile(wait, 99)) if wait.size else None,
+        if gen_pool is not None:
+            gen_pool.shutdown(wait=True)
+        part = {"records": [record(r) for r in requests], "wall_s": wall, "cell_updates": self.cell_updates,
+                "inputs_late": late_inputs if gen_pool is not None else None,
                 "peak_device_bytes": self.peak_used, "peak_members": self.peak_members,
                 "batch_step_s": self.gpu_busy}
+        self.last_part = part  # this server's records, for merging with other ranks' (summarize)
+        return summarize([part])
+
+
+def record(r: Request) -> dict:
+    """The times and work of one served request (seconds from the start of
+    its server's run)."""
+    return {"rid": r.rid, "arrival": r.arrival, "prep_start": r.prep_start, "prepared": r.prepared,
+            "admitted": r.admitted, "done": r.done, "cells": r.cells, "steps": r.steps}
+
+
+def summarize(parts: List[dict]) -> dict:
+    """Throughput and latency of one or more servers' runs (one part per
+    rank, each serving its share of one request stream): latency
+    percentiles over every request, with its parts; throughput = all cell
+    updates / the slowest server's wall time; offered load = the cell
+    updates the requests asked for / the arrival window."""
+    recs = [x for p in parts for x in p["records"]]
+    done = [x for x in recs if x["done"] is not None]
+
+    def pct(vals):
+        a = np.array(vals, dtype=np.float64)
+        return ({"p50_s": float(np.percentile(a, 50)), "p99_s": float(np.percentile(a, 99))}
+                if a.size else {"p50_s": None, "p99_s": None})
+
+    wall = max(p["wall_s"] for p in parts)
+    updates = sum(p["cell_updates"] for p in parts)
+    window = max((x["arrival"] for x in recs), default=0.0)
+    offered = sum(x["steps"] * x["cells"] for x in done)
+    lat = pct([x["done"] - x["arrival"] for x in done])
+    late = [p["inputs_late"] for p in parts if p.get("inputs_late") is not None]
+    return {"requests": len(recs), "completed": len(done), "servers": len(parts), "wall_s": wall,
+            "cell_updates": updates, "cell_updates_per_s": updates / wall if wall > 0 else 0.0,
+            "arrival_window_s": window,
+            "offered_cell_updates_per_s": offered / window if window > 0 else None,
+            "p50_s": lat["p50_s"], "p99_s": lat["p99_s"],
+            "latency_parts": {
+                "admission_wait": pct([x["prep_start"] - x["arrival"] for x in done]),
+                "preparation": pct([x["prepared"] - x["prep_start"] for x in done]),
+                "join_wait": pct([x["admitted"] - x["prepared"] for x in done]),
+                "device_residency": pct([x["done"] - x["admitted"] for x in done])},
+            "inputs_late": sum(late) if late else None,
+            "peak_device_bytes": max(p["peak_device_bytes"] for p in parts),
+            "peak_members": max(p["peak_members"] for p in parts),
+            "batch_step_s": max(p["batch_step_s"] for p in parts)}
+
+
+def shard(requests: List[Request], rank: int, world: int) -> List[Request]:
+    """This rank's share of a request stream: request id modulo the number
+    of ranks. Every request belongs to exactly one rank, and the shares'
+    sizes differ by at most one."""
+    return [r for r in requests if r.rid % world == rank]
 
 
 def poisson_requests(rate: float, duration: float, seed: int, *, n_min: int = 128, n_max: int = 4096,
