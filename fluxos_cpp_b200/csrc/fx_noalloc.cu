@@ -2,28 +2,39 @@
 // allocates no memory at all.
 //
 // Who needs it: callers that are not allowed to call cudaMalloc while they
-// run. Examples are a host model that hands out all of its device memory from
-// its own pool or arena and must stay inside that budget, code that runs
-// while a CUDA graph is being recorded or under a memory-capped job, and
-// coupling layers (the role OpenWQ plays next to FLUXOS) that own the solute
-// arrays and only want the transport step applied to them. Such callers pass
-// device pointers they already hold; this entry point then creates no context,
-// stream or buffer.
+// run. A host model that hands out all of its device memory from its own pool
+// or arena must stay inside that budget, and a job under a hard memory cap may
+// not grow; coupling layers (the role OpenWQ plays next to FLUXOS) own the
+// solute arrays and only want the transport step applied to them. Such
+// callers pass device pointers they already hold; this entry point then
+// creates no context, stream or buffer of its own.
 //
 // The sweep needs scratch memory: per strip of 30 rows, the hand-over values
 // of the strip's last row (3 doubles per column) and a progress counter, plus
-// a small control block. Here that scratch is the file-scope device array
-// g_noalloc_scratch of FX_NOALLOC_SCRATCH_BYTES (8 MiB), which every GPU that
-// loads the library holds until the process exits. Grids whose scratch does
-// not fit are rejected (FX_ERR_ARG).
+// the domain descriptor, the strip table and a control block. Here that
+// scratch is the file-scope device array g_noalloc_scratch of
+// FX_NOALLOC_SCRATCH_BYTES (8 MiB), which every GPU that loads the library
+// holds until the process exits. A grid fits when
+// ceil(nrows / 30) * (ncols + 2) * 24 bytes plus the fixed part (a few KiB)
+// is at most 8 MiB (square grids up to about 3,200 x 3,200 cells); larger
+// grids are rejected with FX_ERR_ARG and a message giving the bytes needed.
 //
-// On each device, the first call looks up the device address of that array
-// (cudaGetSymbolAddress, with the device current) and the sweep kernel's
-// launch limits; make that first call before any stream capture. Every call
-// shares the one array: calls that overlap on the GPU (other streams, other
-// host threads) race on it and must be serialised by the caller. Each call
-// clears the progress counters and rewrites the control block, the only
-// scratch that must start from a known value.
+// Set-up: the first call on a device, with that device current, looks up the
+// device address of the array (cudaGetSymbolAddress; the array's name in host
+// code is only a host-side stand-in) and the sweep kernel's launch limits, and
+// keeps them for that device's CUDA context. A later call repeats the set-up
+// only if the device's context has changed (after cudaDeviceReset the module,
+// and with it the array, is loaded anew). Make the first call on each device
+// before any stream capture.
+//
+// Every call shares the one array: calls that overlap on the GPU (other
+// streams, other host threads) race on it and must be serialised by the
+// caller. The array keeps the last call's contents; each call clears the
+// progress counters and rewrites the descriptor, strip table and control
+// block, the only scratch that must start from a known value (the hand-over
+// values are written before they are read). The call reads the sweep's error
+// flag back and synchronises its stream before it returns.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -52,11 +63,43 @@ constexpr size_t kDevBytes = (sizeof(fx_dev) + 255) & ~(size_t)255;  // fx_dev, 
 
 struct DeviceSetup {
   bool ready = false;
+  unsigned long long ctx_id = 0;     // the CUDA context the set-up belongs to
   unsigned char* scratch = nullptr;  // device address of g_noalloc_scratch
   int max_blocks = 0;
 };
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mutex;
+
+// The unique id of the calling thread's current CUDA context (0: none, or the
+// driver cannot tell). Context ids are never reused within a process, so a
+// changed id means the module and its static array were loaded anew. The two
+// driver calls are reached through the runtime, so libcuda is not linked.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {
+    void* a = nullptr;
+    void* b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+        qa == cudaDriverEntryPointSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+        qb == cudaDriverEntryPointSuccess) {
+      get_current = reinterpret_cast<CtxGetCurrentFn>(a);
+      get_id = reinterpret_cast<CtxGetIdFn>(b);
+    }
+    cudaGetLastError();
+    resolved = true;
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 // Writes the scratch's control block, domain descriptor and work table: one
 // sweep with it > 1 (the ADE is skipped on the first solver iteration,
@@ -118,10 +161,16 @@ extern "C" int fx_adesolver_noalloc(double* conc, const double* h, const double*
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fx_fail(nullptr, FX_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return fx_fail(nullptr, FX_ERR_ARG, "device index %d out of range", dev);
+  DeviceSetup s;
   {
+    // set-up once per device and context, with the device current: the
+    // device address of the static array (its host-side name is not one)
+    // and the sweep kernel's resident blocks
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    DeviceSetup& s = g_setup[dev];
-    if (!s.ready) {
+    DeviceSetup& g = g_setup[dev];
+    const unsigned long long ctx = current_context_id();
+    if (!g.ready || ctx == 0 || ctx != g.ctx_id) {
+      g.ready = false;
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p)
@@ -130,12 +179,13 @@ extern "C" int fx_adesolver_noalloc(double* conc, const double* h, const double*
       int mb = 0;
       if (fx_ade_max_blocks(&mb) != 0 || mb < 1)
         return fx_fail(nullptr, FX_ERR_CUDA, "occupancy query for the ADE sweep failed");
-      s.scratch = (unsigned char*)p;
-      s.max_blocks = mb;
-      s.ready = true;
+      g.scratch = (unsigned char*)p;
+      g.max_blocks = mb;
+      g.ctx_id = current_context_id();  // the look-up made the device's context current
+      g.ready = true;
     }
+    s = g;
   }
-  const DeviceSetup& s = g_setup[dev];
   cudaStream_t st = (cudaStream_t)stream;
 
   fx_dev d;

@@ -218,11 +218,14 @@ int fx_batch_autotune(fx_batch* b, int trial_steps, int* tile_rows, int* steps_i
  * holds one byte per cell: bit 0 ldry, bit 1 ldry_prev, bit 2 wall. h, h0,
  * fe_1, fn_1 are the depth after and before the hydrodynamic update and the
  * face fluxes of that update; dtfl is its time step. The call allocates
- * nothing: its scratch is one static 8 MiB device array per GPU, so grids
- * needing more (about 2,900 x 2,900 cells and up) return FX_ERR_ARG. The
- * first call on a device also looks up that array's device address (do it
- * before any stream capture). All calls share the array and calls that
- * overlap on the GPU race. stream NULL = the default stream; the call returns
+ * nothing: its scratch is one static 8 MiB device array per GPU. A grid fits
+ * when ceil(nrows/30) * (ncols+2) * 24 bytes plus a fixed part of a few KiB
+ * is at most 8 MiB (square grids up to about 3,200 x 3,200 cells); larger
+ * grids return FX_ERR_ARG. The first call on a device (and the first after
+ * its CUDA context is replaced, e.g. by cudaDeviceReset) looks up that
+ * array's device address; make the first call before any stream capture.
+ * All calls share the array and calls that overlap on the GPU race. stream
+ * NULL = the default stream; the call synchronises the stream and returns
  * when the sweep has finished. */
 int fx_adesolver_noalloc(double* conc, const double* h, const double* h0, const unsigned char* flags,
                          const double* fe_1, const double* fn_1, int nrows, int ncols, int ld, int dxy,
