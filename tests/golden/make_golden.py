@@ -11,6 +11,15 @@ snapshots are saved at the listed step counts. Two cases also keep the
 Results/<t>.txt files that the whole reference program (oracle/_ref/fluxos_ref)
 writes. The fixtures hold the input text, so tests need neither the reference
 nor this script.
+
+The case ``c1_plane200`` is the small CPU configuration run in full by the
+reference program: 200 x 200 cells of 2 m, a plane sloping 0.01 with smoothed
+Gaussian bumps (seed 0), dry start, 20 mm/day of melt at 1 mg/L for 6 h,
+D = 0.01 m^2/s, output every 600 s (36 Results files). Its 124 MB of text is
+kept as digests (tests/results_digest.py: SHA-256, row set, wet-cell count,
+column sums, sample rows) plus every value of the files at 10,200 s and
+21,600 s, and the SHA-256 of the input files, which
+scenarios.plane_scenario() regenerates.
 """
 from __future__ import annotations
 
@@ -183,6 +192,47 @@ def build_case(name: str, spec: dict) -> None:
     print(name, "snapshots", spec["steps"], "results" if spec["results"] else "")
 
 
+C1_FULL = ("10200.txt", "21600.txt")
+
+
+def build_c1() -> None:
+    """The small CPU configuration through the whole reference program."""
+    import hashlib
+    sys.path.insert(0, os.path.dirname(HERE))
+    import results_digest as RD
+    sc = S.plane_scenario()
+    work = tempfile.mkdtemp(prefix="golden_c1_")
+    modset = sc.write(work)
+    r = subprocess.run([P.REF_BIN, modset], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr)
+    res = os.path.join(work, "Results")
+    files = sorted(os.listdir(res), key=lambda s: int(s.split(".")[0]))
+    meta = dict(name="c1_plane200", nrows=sc.nrows, ncols=sc.ncols, dxy=sc.dxy, ks=sc.ks,
+                horizon=sc.horizon, print_step=sc.print_step, results=files, full=list(C1_FULL),
+                inputs={})
+    for fn in ("dem.asc", "meteo.csv"):
+        with open(os.path.join(work, fn), "rb") as f:
+            meta["inputs"][fn] = hashlib.sha256(f.read()).hexdigest()
+    out = {}
+    meta["digest"] = {}
+    for k, fn in enumerate(files):
+        with open(os.path.join(res, fn)) as f:
+            text = f.read()
+        dg = RD.digest(text, sc.nrows, sc.ncols, seed=k, hdry=sc.ks)
+        meta["digest"][fn] = {"sha256": dg["sha256"], "header": dg["header"], "rows": dg["rows"],
+                              "wet": dg["wet"]}
+        t = fn.split(".")[0]
+        out[f"mask_{t}"] = dg["mask"]
+        out[f"sums_{t}"] = dg["sums"]
+        out[f"samples_{t}"] = dg["samples"]
+        if fn in C1_FULL:
+            out[f"full_{t}"] = RD.full_columns(text)
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "c1_plane200.npz"), **out)
+    print("c1_plane200", len(files), "Results files")
+
+
 def main() -> None:
     if not P.ref_available(0):
         sys.exit("oracle/_ref is not built: run `make -C oracle all REF=<FLUXOS_cpp tree>`")
@@ -190,6 +240,8 @@ def main() -> None:
     for name, fn in CASES.items():
         if not only or name in only:
             build_case(name, fn())
+    if not only or "c1_plane200" in only:
+        build_c1()
 
 
 if __name__ == "__main__":
