@@ -31,7 +31,16 @@ Also reported on the same line (skipped with --no-mix / --no-serve):
   and discharge error of FP32 against FP64, both water balances;
 * results_writer (--no-writer): one Results file of the headline state
   written from rows compacted on the device, asynchronously, and by the
-  host writer from downloaded grids (text into /dev/null).
+  host writer from downloaded grids (text into /dev/null);
+* c1 (--no-c1): the small CPU configuration (200 x 200 plane with bumps, dry
+  start, 6 h of melt, 36 Results files) run in full: the drop-in program
+  fluxos_gpu (FP64) end to end, the same run's stepping timed on the device,
+  and the reference program (oracle/_ref) on all host cores;
+* parity_crop (with the CPU leg): the GPU FP64 path in parity mode on
+  exactly the crop the reference times (2048^2, uniform melt at the field
+  mean, no Manning, the same wet start), its state compared cell by cell with
+  the reference's after the same steps, and its rate beside the reference's:
+  the like-for-like ratio.
 
 --impl reference times the FLUXOS reference sources compiled in oracle/_ref
 (OpenMP hydrodynamics, serial ADE) on the host cores instead.
@@ -41,6 +50,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -63,7 +73,9 @@ METRIC = "cell-updates/s FP32 vs FP64 at stated depth/mass error; p50/p99 reques
 # FP64 bed: 49 B of hydro state); the roofline's `traffic` field gives what
 # the kernel actually moved.
 ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
-             "fp32": {"k_hydro": 37, "k_ade_sweep": 8, "step": 45}}
+             "fp32": {"k_hydro": 37, "k_ade_sweep": 8, "step": 45},
+             # parity mode (no Manning n, no melt field): 2*8*3 + 8 + 1 = 57 B hydro
+             "fp64_parity": {"k_hydro": 57, "k_ade_sweep": 16, "step": 73}}
 # DRAM bytes per cell that each kernel actually moves per step
 # (dram__bytes_read.sum + dram__bytes_write.sum from ncu on the 2048 x 2048
 # case of this workload, one launch, divided by the cells and the steps the
@@ -290,19 +302,29 @@ class _stdout_to_stderr:
         return False
 
 
-def cpu_reference_run(sc, h, conc, warmup: int, steps: int, crop: int):
+def crop_scenario(sc, crop: int):
+    """A square crop of the workload in parity mode: the reference has no
+    melt field and no Manning term, so the melt is the field's mean rate,
+    uniform, and there is no friction."""
+    from fluxos_cpp_b200 import scenarios as S
+    n = min(crop, sc.nrows)
+    return S.Scenario(name=f"crop{n}", dem=sc.dem[:n, :n].copy(), dxy=sc.dxy, meteo=sc.meteo,
+                      horizon=sc.horizon, print_step=sc.print_step, ks=sc.ks, ade=True, d_coef=sc.d_coef)
+
+
+def cpu_reference_run(sc, h, conc, warmup: int, steps: int, crop: int, keep: bool = False):
     """The reference sources (oracle/_ref) on a crop of the same workload,
-    in parity mode (the reference has no melt field and no Manning term)."""
+    in parity mode. With keep, the result also holds the reference run (its
+    state after warmup + steps steps) and the crop's input folder, which the
+    caller removes."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as P
-    from fluxos_cpp_b200 import scenarios as S
     if not P.ref_available(0):
         return None
-    n = min(crop, sc.nrows)
-    sub = S.Scenario(name=f"crop{n}", dem=sc.dem[:n, :n].copy(), dxy=sc.dxy,
-                     meteo=sc.meteo, horizon=sc.horizon, print_step=sc.print_step, ks=sc.ks,
-                     ade=True, d_coef=sc.d_coef)
-    with tempfile.TemporaryDirectory() as tmp, _stdout_to_stderr():
+    sub = crop_scenario(sc, crop)
+    n = sub.nrows
+    tmp = tempfile.mkdtemp(prefix="fluxos_crop_")
+    with _stdout_to_stderr():
         mp = sub.write(tmp)
         ref = P.RefRun(mp, sub, 0)
         ref.apply_wet_start(h[:n, :n], None, None, [conc[:n, :n]])
@@ -313,12 +335,149 @@ def cpu_reference_run(sc, h, conc, warmup: int, steps: int, crop: int):
             ref.step()
         t1 = time.perf_counter()
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": n * n * steps / (t1 - t0), "unit": "cell-updates/s", "cores": threads,
-            "kind": "reference", "seconds": t1 - t0,
-            "sample": f"{n}x{n} crop of the workload (uniform melt at the field mean, no Manning: "
-                      f"the reference has neither), {warmup} warm-up + {steps} timed steps, "
-                      f"reference sources from oracle/_ref, OpenMP hydrodynamics on {threads} threads, "
-                      f"serial ADE"}
+    out = {"value": n * n * steps / (t1 - t0), "unit": "cell-updates/s", "cores": threads,
+           "kind": "reference", "seconds": t1 - t0,
+           "sample": f"{n}x{n} crop of the workload (uniform melt at the field mean, no Manning: "
+                     f"the reference has neither), {warmup} warm-up + {steps} timed steps, "
+                     f"reference sources from oracle/_ref, OpenMP hydrodynamics on {threads} threads, "
+                     f"serial ADE"}
+    if keep:
+        out.update(_ref=ref, _dir=tmp, _modset=mp, _sub=sub)
+    else:
+        del ref
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
+
+
+PARITY_FIELDS = ("z", "h", "qx", "qy", "conc", "twet", "h0", "fe_1", "fe_2", "fe_3", "fn_1", "fn_2", "fn_3")
+
+
+def run_parity_crop(cpu: dict, h, conc, steps: int, in_flight: int, peak: float) -> dict:
+    """The GPU FP64 path on the reference's crop, from the same input files
+    and the same wet start: after the reference's warm-up + timed steps, the
+    largest relative difference per field (floored at 1e-6 of the field's
+    largest magnitude) and the wet/dry flags that differ; then `steps` steps
+    timed with CUDA events beside the reference's rate."""
+    import fluxos_cpp_b200 as fx
+    ref, sub, mp = cpu["_ref"], cpu["_sub"], cpu["_modset"]
+    n = sub.nrows
+    ncmp = int(ref.scalar("it"))
+    d = fx.Domain.from_modset_state(mp, steps_in_flight=in_flight)
+    try:
+        # the wet start exactly as the reference run got it (RefRun.apply_wet_start)
+        zb, z, hh, cc = d.download("zb"), d.download("z"), d.download("h"), d.download("conc")
+        hh[1:-1, 1:-1] = h[:n, :n].T
+        z[1:-1, 1:-1] = zb[1:-1, 1:-1] + h[:n, :n].T
+        cc[1:-1, 1:-1] = conc[:n, :n].T
+        for k, g in (("z", z), ("h", hh), ("conc", cc)):
+            d.upload(k, g)
+        fl = d.download_flags()
+        ld = fl["ldry"].copy()
+        ld[1:-1, 1:-1] = np.where(h[:n, :n].T > 0, 0.0, 1.0)
+        d.upload_flags(ld, fl["wall"])
+        d.prepare()
+        done = 0
+        while done < ncmp:
+            st = d.step(ncmp - done)
+            done = int(st["it"])
+            if st["finished"]:
+                break
+        errs = {}
+        for k in PARITY_FIELDS:
+            a, b = ref.grid(k)[1:-1, 1:-1], d.download(k)[1:-1, 1:-1]
+            scale = max(float(np.abs(a).max()), 1e-300) * 1e-6
+            errs[k] = 0.0 if np.array_equal(a, b) else float(
+                (np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), scale)).max())
+        fl = d.download_flags()
+        flags_differ = int((fl["ldry"][1:-1, 1:-1] != ref.grid("ldry")[1:-1, 1:-1]).sum())
+        tim_equal = d.status()["tim"] == ref.scalar("tim")
+        ms, ms_h, ms_a = d.time_steps(steps)
+        gpu_rate = n * n * steps / (ms / 1e3)
+    finally:
+        d.close()
+        del cpu["_ref"]
+        shutil.rmtree(cpu.pop("_dir"), ignore_errors=True)
+        cpu.pop("_modset")
+        cpu.pop("_sub")
+    return {"cells": n * n, "steps_compared": ncmp, "max_rel_err": errs,
+            "max_rel_err_all": max(errs.values()), "flags_differ": flags_differ, "clock_equal": bool(tim_equal),
+            "gpu_fp64_cell_updates_per_s": gpu_rate, "gpu_ms_per_step": ms / steps,
+            "gpu_ms_per_step_hydro_ade": [round(ms_h / steps, 4), round(ms_a / steps, 4)],
+            "gpu_alg_GBps": round(gpu_rate * ALG_BYTES["fp64_parity"]["step"] / 1e9, 1),
+            "gpu_hbm_frac": round(gpu_rate * ALG_BYTES["fp64_parity"]["step"] / 1e9 / peak, 4),
+            "cpu_reference_cell_updates_per_s": cpu["value"], "cpu_cores": cpu["cores"],
+            "gpu_over_cpu": round(gpu_rate / cpu["value"], 1),
+            "note": "same input files, same wet start, FP64 on both sides, parity mode (uniform melt, no "
+                    "Manning); state compared after the reference's warm-up + timed steps; GPU rate from "
+                    f"{steps} further steps timed with CUDA events (state larger than L2)"}
+
+
+def run_c1(args) -> dict:
+    """The small CPU configuration run in full: 200 x 200 cells of 2 m, dry
+    start, 20 mm/day for 6 h, 36 Results files. The drop-in program
+    fluxos_gpu (FP64, files written) end to end; the same run's stepping on
+    the device alone (a context from the same modset, run to each output, no
+    files; CUDA events on the context's stream); the reference program
+    (oracle/_ref/fluxos_ref, OpenMP on all host cores) end to end."""
+    import torch
+    import fluxos_cpp_b200 as fx
+    from fluxos_cpp_b200 import scenarios as S
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as P
+    sc = S.plane_scenario()
+    cells = sc.nrows * sc.ncols
+    out = {"workload": "plane 200x200 cells of 2 m with smoothed bumps (seed 0), dry start, 20 mm/day "
+                       "for 6 h at 1 mg/L, D 0.01 m^2/s, output every 600 s (36 Results files)",
+           "precision": "fp64 (the reference's arithmetic)"}
+    with tempfile.TemporaryDirectory() as tmp:
+        mp = sc.write(tmp)
+        t0 = time.perf_counter()
+        r = subprocess.run([fx.EXE_PATH, mp], capture_output=True, text=True)
+        out["gpu_program_s"] = round(time.perf_counter() - t0, 3)
+        if r.returncode != 0:
+            raise RuntimeError("fluxos_gpu failed: " + r.stderr[-500:])
+        out["results_files"] = len(os.listdir(os.path.join(tmp, "Results")))
+        d = fx.Domain.from_modset_state(mp, steps_in_flight=args.c1_in_flight)
+        stream = torch.cuda.ExternalStream(d.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(stream)
+        while True:
+            st = d.run_to_print()
+            if st["print_pending"]:
+                d.print_done()
+                continue
+            if st["finished"]:
+                break
+        e1.record(stream)
+        torch.cuda.synchronize()
+        host_s = time.perf_counter() - t0
+        it, steps = int(st["it"]), int(st["steps"])
+        d.close()
+        updates = it * cells  # cells advanced in every step the solver runs (hpall != 0)
+        out.update({"iterations": steps, "solver_iterations": it, "cell_updates": updates,
+                    "steps_in_flight": args.c1_in_flight,
+                    "gpu_steps_device_s": round(e0.elapsed_time(e1) / 1e3, 4),
+                    "gpu_steps_host_s": round(host_s, 4),
+                    "gpu_cell_updates_per_s": updates / (e0.elapsed_time(e1) / 1e3),
+                    "gpu_program_cell_updates_per_s": updates / out["gpu_program_s"]})
+        if P.ref_available(0) and not args.no_c1_ref:
+            ref_dir = os.path.join(tmp, "ref")
+            mp2 = sc.write(ref_dir)
+            threads = os.cpu_count() or 1
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            t0 = time.perf_counter()
+            r = subprocess.run([P.REF_BIN, mp2], capture_output=True, text=True, env=env)
+            ref_s = time.perf_counter() - t0
+            if r.returncode == 0:
+                out.update({"reference_program_s": round(ref_s, 3), "reference_cores": threads,
+                            "reference_cell_updates_per_s": updates / ref_s,
+                            "gpu_program_over_reference": round(ref_s / out["gpu_program_s"], 1)})
+    out["note"] = ("program times are wall clock of the whole process (start-up, 46k steps, 36 files of "
+                   "text); the state (2 MB) is L2-resident, so the GPU stepping is launch-bound, not a "
+                   "roofline case")
+    return out
 
 
 def measure_domain(d, steps: int, warmup: int, cells: int, precision: str, peak: float, gpu: str,
@@ -369,6 +528,32 @@ def accuracy_of(d32, d64, w32: float, w64: float, hdry: float) -> dict:
             "mass_balance_rel_fp32": b32["rel_err"], "mass_balance_rel_fp64": b64["rel_err"]}
 
 
+def mix_accuracy(st32: list, st64: list) -> dict:
+    """FP32 batch against FP64 batch, member by member after the same steps:
+    relative L1 and absolute L-infinity depth and discharge error (|q|), per
+    member and over all members, and both precisions' water balances."""
+    per, num_h, den_h, num_q, den_q = [], 0.0, 0.0, 0.0, 0.0
+    linf_h = linf_q = 0.0
+    for a, b in zip(st32, st64):
+        dh, dq = np.abs(a["h"] - b["h"]), np.abs(a["q"] - b["q"])
+        sh, sq = float(np.abs(b["h"]).sum()), float(np.abs(b["q"]).sum())
+        num_h, den_h, num_q, den_q = num_h + float(dh.sum()), den_h + sh, num_q + float(dq.sum()), den_q + sq
+        linf_h, linf_q = max(linf_h, float(dh.max())), max(linf_q, float(dq.max()))
+        per.append({"depth_l1_rel": float(dh.sum()) / sh if sh else 0.0, "depth_linf_m": float(dh.max()),
+                    "discharge_l1_rel": float(dq.sum()) / sq if sq else 0.0,
+                    "same_steps": a["steps"] == b["steps"], "tim_fp32": a["tim"], "tim_fp64": b["tim"]})
+    d_l1 = [p["depth_l1_rel"] for p in per]
+    return {"against": "the FP64 batch (each member the reference's arithmetic) after the same steps",
+            "depth_l1_rel": num_h / den_h, "depth_linf_m": linf_h,
+            "discharge_l1_rel": num_q / den_q, "discharge_linf_m2s": linf_q,
+            "depth_l1_rel_per_member": {"max": max(d_l1), "median": float(np.median(d_l1)),
+                                        "all": [float(f"{x:.3g}") for x in d_l1]},
+            "discharge_l1_rel_max_member": max(p["discharge_l1_rel"] for p in per),
+            "members_with_equal_steps": sum(p["same_steps"] for p in per),
+            "mass_balance_rel_fp32_max": max(a["mass_rel_err"] for a in st32),
+            "mass_balance_rel_fp64_max": max(b["mass_rel_err"] for b in st64)}
+
+
 def run_mix(args, peak: float) -> dict:
     """The 64-scenario ensemble: FP32 batch vs FP64 batch vs FP64 one by one."""
     import torch
@@ -384,8 +569,10 @@ def run_mix(args, peak: float) -> dict:
     def batch_rate(precision):
         # FP32 members hold 63 steps in flight (82 GB for the 64 scenarios); FP64 ones
         # args.mix_in_flight (memory: FP64 slot planes are twice as large)
+        from fluxos_cpp_b200 import accuracy as A
         k_members = 63 if precision == "fp32" else args.mix_in_flight
         doms = [S.make_domain(sc, precision=precision, steps_in_flight=k_members) for sc in scs]
+        w0 = [d.mass()[0] for d in doms]
         b = fx.Batch()
         for d in doms:
             b.add(d)
@@ -404,13 +591,24 @@ def run_mix(args, peak: float) -> dict:
         ms = e0.elapsed_time(e1)
         done = sum((d.status()["steps"] - a) * c for d, a, c in zip(doms, s0, cells))
         nbytes = sum(d.device_bytes() for d in doms)
+        # the members' states after the timed steps (interior depth and
+        # discharge on the host) and their water balances, for the error of
+        # FP32 against FP64
+        states = []
+        for d, w in zip(doms, w0):
+            st = d.status()
+            states.append({"h": d.download("h")[1:-1, 1:-1].copy(),
+                           "q": np.hypot(d.download("qx")[1:-1, 1:-1], d.download("qy")[1:-1, 1:-1]),
+                           "steps": int(st["steps"]), "tim": st["tim"],
+                           "mass_rel_err": A.water_balance(d, w)["rel_err"]})
         b.close()
         for d in doms:
             d.close()
-        return done / (ms / 1e3), ms, tuned, nbytes
+        return done / (ms / 1e3), ms, tuned, nbytes, states
 
-    r32, ms32, tuned, bytes32 = batch_rate("fp32")
-    r64b, ms64b, _, bytes64 = batch_rate("fp64")
+    r32, ms32, tuned, bytes32, st32 = batch_rate("fp32")
+    r64b, ms64b, _, bytes64, st64 = batch_rate("fp64")
+    acc = mix_accuracy(st32, st64)
     # plain FP64 path: each scenario alone, one after another
     tot_ms, tot_cells = 0.0, 0
     for sc, c in zip(scs, cells):
@@ -432,7 +630,7 @@ def run_mix(args, peak: float) -> dict:
             "fp32_batch_over_fp64_batch": round(r32 / r64b, 3),
             "autotuned": {"tile_rows": tuned[0], "steps_in_flight": tuned[1]},
             "device_bytes_fp32": bytes32, "device_bytes_fp64": bytes64,
-            "host_generation_s": round(gen_s, 1),
+            "host_generation_s": round(gen_s, 1), "accuracy": acc,
             "note": "per-scenario dt; timed region = one fx_batch_step of all members (CUDA events on "
                     "the batch stream); plain FP64 = each scenario alone through fx_time_steps"}
 
@@ -455,33 +653,97 @@ def front_radii(d, sc, hdry: float) -> list:
     return out
 
 
+def _perturbed(sc, seed: int):
+    """An FP64 domain of the scenario whose initial depths are perturbed by
+    a relative 1e-7 (seeded, uniform in [-1, 1]): about one FP32 rounding."""
+    from fluxos_cpp_b200 import scenarios as S
+    d = S.make_domain(sc, precision="fp64", steps_in_flight=31)
+    h, z = d.download("h"), d.download("z")
+    dh = h * 1e-7 * np.random.default_rng(seed).uniform(-1, 1, h.shape)
+    d.upload("h", h + dh)
+    d.upload("z", z + dh)
+    d.prepare()
+    return d
+
+
+def _linf_at(a, b, sc) -> dict:
+    """Where |a - b| of two interior depth grids is largest: the cell, its
+    distance from the grid centre and both depths."""
+    diff = np.abs(a - b)
+    ic, ir = np.unravel_index(int(np.argmax(diff)), diff.shape)  # [icol - 1, irow - 1]
+    x, y = (ic + 0.5) * sc.dxy - sc.ncols * sc.dxy / 2, (ir + 0.5) * sc.dxy - sc.nrows * sc.dxy / 2
+    return {"irow": int(ir) + 1, "icol": int(ic) + 1, "r_m": round(float(np.hypot(x, y)), 2),
+            "abs": float(diff[ic, ir]), "depth_test": float(a[ic, ir]), "depth_ref": float(b[ic, ir])}
+
+
 def run_dambreak(args) -> dict:
     """The circular dam break (2048^2 cells of 1 m, 2 m of water within 300 m
     of the centre, flat bed, Manning n 0.02, two solutes, 600 s): FP32 against
     FP64 at the horizon, with the front position along 8 rays and both water
-    balances."""
+    balances. Two FP64 runs whose initial depths are perturbed by a relative
+    1e-7 give the scheme's own sensitivity to one rounding (the envelope the
+    FP32 error is read against); every 60 s of the run the depth error of
+    FP32 and of the perturbed runs against FP64 is recorded, with the cell of
+    the largest difference."""
     from fluxos_cpp_b200 import accuracy as A
     from fluxos_cpp_b200 import scenarios as S
     n = args.dambreak_size
     sc = S.dambreak_scenario(n, dxy=1, radius=300.0 * n / 2048, depth=2.0, base=100.0,
                              horizon=args.dambreak_horizon)
+    sc.print_step = int(min(60, sc.horizon))
     out = {"cells": n * n, "horizon_s": sc.horizon, "radius_m": sc.extra["radius"]}
     doms, w0 = {}, {}
     for p in ("fp64", "fp32"):
-        d = S.make_domain(sc, precision=p, steps_in_flight=31)
-        w0[p] = d.mass()[0]
-        t0 = time.perf_counter()
-        st = d.run_to_print()  # one output, at the horizon
-        out[f"{p}_steps"] = st["steps"]
-        out[f"{p}_wall_s"] = round(time.perf_counter() - t0, 3)
+        doms[p] = S.make_domain(sc, precision=p, steps_in_flight=31)
+        w0[p] = doms[p].mass()[0]
+    pert = [_perturbed(sc, seed) for seed in (0, 1)] if not args.no_envelope else []
+    history = []
+    wall = {"fp64": 0.0, "fp32": 0.0}
+    while True:
+        for p in ("fp64", "fp32"):
+            t0 = time.perf_counter()
+            doms[p].run_to_print()
+            wall[p] += time.perf_counter() - t0
+        for d in pert:
+            d.run_to_print()
+        t_out = doms["fp64"].status()["tim"]
+        h64 = doms["fp64"].download("h")[1:-1, 1:-1]
+        h32 = doms["fp32"].download("h")[1:-1, 1:-1]
+        rec = {"t": round(t_out, 3), "fp32_depth_l1_rel": float(np.abs(h32 - h64).sum() / np.abs(h64).sum()),
+               "fp32_linf": _linf_at(h32, h64, sc)}
+        if pert:
+            hp = [d.download("h")[1:-1, 1:-1] for d in pert]
+            rec["perturbed_depth_l1_rel"] = [float(np.abs(x - h64).sum() / np.abs(h64).sum()) for x in hp]
+            rec["perturbed_linf"] = [_linf_at(x, h64, sc) for x in hp]
+        history.append(rec)
+        if all(d.status()["finished"] or d.status()["tim"] >= sc.horizon for d in doms.values()):
+            break
+        for d in list(doms.values()) + pert:
+            if d.status()["print_pending"]:
+                d.print_done()
+    for p in ("fp64", "fp32"):
+        st = doms[p].status()
+        out[f"{p}_steps"] = int(st["steps"])
+        out[f"{p}_wall_s"] = round(wall[p], 3)
         out[f"{p}_tim"] = st["tim"]
-        doms[p] = d
     e = A.state_errors(doms["fp32"], doms["fp64"], sc.ks)
     out["depth_l1_rel"] = e["depth"]["l1_rel"]
     out["depth_linf_abs"] = e["depth"]["linf_abs"]
     out["discharge_l1_rel"] = e["discharge"]["l1_rel"]
     out["wet_cells_differ"] = e["wet_cells"]["differ"]
     out["solute_mass_l1_rel"] = [c["l1_rel"] for c in e["solute_mass_density"]]
+    out["depth_linf_at"] = history[-1]["fp32_linf"]
+    if pert:
+        ep = [A.state_errors(d, doms["fp64"], sc.ks) for d in pert]
+        out["envelope"] = {"what": "two FP64 runs with initial depths perturbed by a relative 1e-7, "
+                                   "against the unperturbed FP64 run",
+                           "depth_l1_rel": [x["depth"]["l1_rel"] for x in ep],
+                           "depth_linf_abs": [x["depth"]["linf_abs"] for x in ep],
+                           "discharge_l1_rel": [x["discharge"]["l1_rel"] for x in ep],
+                           "wet_cells_differ": [x["wet_cells"]["differ"] for x in ep]}
+        lim = max(out["envelope"]["depth_l1_rel"])
+        out["fp32_depth_l1_over_envelope"] = round(out["depth_l1_rel"] / lim, 3) if lim > 0 else None
+    out["history"] = history
     for p in ("fp64", "fp32"):
         d = doms[p]
         out[f"{p}_front_m"] = front_radii(d, sc, sc.ks)
@@ -489,6 +751,8 @@ def run_dambreak(args) -> dict:
         out[f"{p}_solute_mass"] = [float(x) for x in d.mass()[1]]
         out[f"{p}_conc_max"] = [float(d.download("conc" if k == 0 else f"conc{k}").max())
                                 for k in range(sc.nchem)]
+        d.close()
+    for d in pert:
         d.close()
     out["note"] = ("the initial concentration is at most 1; the reference's ADE scheme (restated "
                    "bit for bit by the FP64 path) is not bounded at D = 1.0 m^2/s on 1 m cells: "
@@ -498,18 +762,49 @@ def run_dambreak(args) -> dict:
     return out
 
 
-def run_serve(args) -> dict:
+def run_serve(args, rank: int = 0, world: int = 1):
+    """The serving configuration's request stream (Poisson arrivals at
+    4/s, seed 4, grids 128^2-4096^2, 1-12 h horizons, 1-3 solutes, FP32,
+    admission capped at 150 GB) over a bounded arrival window, with the
+    horizons scaled (printed, with the reason); inputs generated ahead of
+    arrival, off the latency clock. With several ranks each serves its share
+    (serve.shard) on its own GPU and rank 0 merges the records. Returns the
+    merged figures on rank 0, None elsewhere."""
+    import torch.distributed as dist
     from fluxos_cpp_b200 import serve
     reqs = serve.poisson_requests(rate=4.0, duration=args.serve_seconds, seed=4,
                                   horizon_scale=args.serve_horizon_scale)
     srv = serve.Server(cap_bytes=150e9, chunk_steps=32)
-    stats = srv.run(reqs)
+    srv.run(serve.shard(reqs, rank, world), generate_ahead=args.serve_generate_ahead, generator_threads=8)
+    part = srv.last_part
     srv.close()
-    stats.update({"arrivals": f"Poisson 4/s for {args.serve_seconds:g} s (seed 4)",
+    if world > 1:
+        parts = [None] * world
+        dist.all_gather_object(parts, part)
+    else:
+        parts = [part]
+    if rank != 0:
+        return None
+    stats = serve.summarize(parts)
+    # the load the configuration's full horizons would offer: the same
+    # requests' measured steps per simulated second, over unscaled horizons
+    full_offer = (stats["offered_cell_updates_per_s"] / args.serve_horizon_scale
+                  if stats["offered_cell_updates_per_s"] else None)
+    stats.update({"arrivals": f"Poisson 4/s for {args.serve_seconds:g} s (seed 4; the configuration: 600 s)",
                   "grids": "128^2..4096^2 log-uniform", "solutes": "1-3",
-                  "horizon": f"1-12 h x {args.serve_horizon_scale:g} (bounded sample)",
+                  "horizon": f"1-12 h x {args.serve_horizon_scale:g}",
+                  "offered_cell_updates_per_s_full_horizons": full_offer,
+                  "horizon_scale_reason": "with 1-12 h horizons the stream offers about "
+                                          f"{(full_offer or 0) / 1e9:.0f} G cell-updates/s, far beyond one "
+                                          "GPU (every request would wait without bound); scaled horizons "
+                                          "keep the arrival process and grid sizes and put the offered load "
+                                          "near the GPU's capacity, so latency measures the solver and the "
+                                          "admission, not an unbounded queue",
                   "admission_cap_bytes": 150e9, "precision": "fp32",
-                  "latency": "arrival to retirement, including host-side input generation"})
+                  "latency": "arrival to retirement; inputs generated ahead of arrival (off the clock); parts: "
+                             "admission wait (arrival to preparation start), preparation (context creation "
+                             "and upload), join wait, device residency (in the batch until retirement)",
+                  "ranks": world})
     return stats
 
 
@@ -563,12 +858,15 @@ def run_gpu(args):
         d.close()
     batches = (args.steps + k_batch - 1) // k_batch
     launches = 2 * args.steps + 2 * batches  # finalize + hydro per step; batch open + sweep per batch
-    cpu = None
+    cpu = crop = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference_run(sc, h, conc, 1, args.cpu_steps, args.cpu_crop)
+        cpu = cpu_reference_run(sc, h, conc, 1, args.cpu_steps, args.cpu_crop, keep=True)
+        if cpu is not None:
+            crop = run_parity_crop(cpu, h, conc, args.steps, k_batch, peak)
+    c1 = run_c1(args) if (rank == 0 and world == 1 and not args.no_c1) else None
     mix = run_mix(args, peak) if (rank == 0 and world == 1 and not args.no_mix) else None
     dam = run_dambreak(args) if (rank == 0 and world == 1 and not args.no_dambreak) else None
-    srv = run_serve(args) if (rank == 0 and world == 1 and not args.no_serve) else None
+    srv = run_serve(args, rank, world) if not args.no_serve else None
     if rank == 0:
         roof = dict(res[head]["roofline"])
         roof["peak_source"] = peak_kind
@@ -583,7 +881,12 @@ def run_gpu(args):
                                                 if head == "fp32" else " (the reference's arithmetic)"),
                            "cells": cells,
                            "l2": "inputs larger than L2 (4-8 GB of state per replica)",
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"replicas x{world}",
+                           "reference_arm": f"the reference's CPU path on a {min(args.cpu_crop, n)}^2 crop "
+                                            "of this workload in parity mode (uniform melt at the field "
+                                            "mean, no Manning), FP64: not this configuration; the "
+                                            "like-for-like GPU rate on that crop is "
+                                            "parity_crop.gpu_fp64_cell_updates_per_s"},
                 "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": res[head]["clocks"],
                 "cpu_baseline": cpu, "accuracy": acc,
                 "autotuned": {"tile_rows": res[head]["tile_rows"]}}
@@ -592,6 +895,10 @@ def run_gpu(args):
                             "autotuned": {"tile_rows": res["fp64"]["tile_rows"]},
                             "roofline": res["fp64"]["roofline"], "clocks": res["fp64"]["clocks"]}
             line["fp32_over_fp64"] = round(res[head]["value"] / res["fp64"]["value"], 3)
+        if crop is not None:
+            line["parity_crop"] = crop
+        if c1 is not None:
+            line["c1"] = c1
         if writer is not None:
             line["results_writer"] = writer
         if mix is not None:
@@ -652,11 +959,21 @@ def main():
                     help="hydrodynamic tile shape (0: autotune)")
     ap.add_argument("--dambreak-size", type=int, default=2048)
     ap.add_argument("--dambreak-horizon", type=float, default=600.0)
+    ap.add_argument("--no-envelope", action="store_true",
+                    help="dam break without the two perturbed FP64 runs")
     ap.add_argument("--mix-count", type=int, default=64)
     ap.add_argument("--mix-steps", type=int, default=62)
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--no-c1", action="store_true", help="skip the small CPU configuration run in full")
+    ap.add_argument("--no-c1-ref", action="store_true",
+                    help="in the c1 section, skip the reference program's full run")
+    ap.add_argument("--c1-in-flight", type=int, default=31,
+                    help="steps in flight of the c1 section's device-timed run")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="arrival window of the serving sample (the configuration's: 600 s)")
     ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 120.0)
+    ap.add_argument("--serve-generate-ahead", type=float, default=3.0,
+                    help="seconds before arrival at which a request's inputs are generated")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -260,6 +260,28 @@ class Domain:
                 h_min_print=info["params"]["h_min_print"], _handle=h)
         return d
 
+    @classmethod
+    def from_modset_state(cls, path: str, *, steps_in_flight: int = 0, precision: str = "fp64") -> "Domain":
+        """A context holding the start-up state of a modset (the state
+        fx_open_modset builds, from the host loader), with the given steps in
+        flight and precision; no output folder is created."""
+        info = load_modset(path)
+        g, p = info["grid"], info["params"]
+        d = cls(g["nrows"], g["ncols"], g["dxy"], nchem=g["nchem"], nodata=g["nodata"], xll=g["xll"],
+                yll=g["yll"], hdry=p["hdry"], ks=p["ks"], ntim=p["ntim"], print_step=p["print_step"],
+                print_next=p["print_next"], tim=p["tim"], h_min_print=p["h_min_print"], ade=bool(p["ade"]),
+                volrat_mode=p["volrat_mode"], d_coef=p["d_coef"][:g["nchem"]],
+                steps_in_flight=steps_in_flight, precision=precision, wintra=bool(p["wintra"]),
+                soil_release_rate=p["soil_release_rate"])
+        for k in ("zb", "z", "h", "qx", "qy", "twet", "conc"):
+            d.upload(k, info[k])
+        if p["wintra"] or info["soil_mass"].any():
+            d.upload("soil_mass", info["soil_mass"])
+        d.upload_flags(info["ldry"], info["wall"])
+        d.set_forcing(info["meteo"] if info["has_meteo"] else None)
+        d.prepare()
+        return d
+
     def close(self) -> None:
         if getattr(self, "h", None):
             self.L.fx_destroy(self.h)
