@@ -364,6 +364,7 @@ def run_parity_crop(cpu: dict, h, conc, steps: int, in_flight: int, peak: float)
     ncmp = int(ref.scalar("it"))
     d = fx.Domain.from_modset_state(mp, steps_in_flight=in_flight)
     try:
+        d.set_option("store_all_fluxes", 1)  # fe_2, fe_3, fn_2, fn_3 of wet cells too, as GlobVar holds them
         # the wet start exactly as the reference run got it (RefRun.apply_wet_start)
         zb, z, hh, cc = d.download("zb"), d.download("z"), d.download("h"), d.download("conc")
         hh[1:-1, 1:-1] = h[:n, :n].T
@@ -566,7 +567,7 @@ def run_mix(args, peak: float) -> dict:
     cells = [sc.nrows * sc.ncols for sc in scs]
     steps = args.mix_steps
 
-    def batch_rate(precision):
+    def batch_rate(precision, match_steps=None):
         # FP32 members hold 63 steps in flight (82 GB for the 64 scenarios); FP64 ones
         # args.mix_in_flight (memory: FP64 slot planes are twice as large)
         from fluxos_cpp_b200 import accuracy as A
@@ -593,7 +594,20 @@ def run_mix(args, peak: float) -> dict:
         nbytes = sum(d.device_bytes() for d in doms)
         # the members' states after the timed steps (interior depth and
         # discharge on the host) and their water balances, for the error of
-        # FP32 against FP64
+        # FP32 against FP64; with match_steps, each member first steps on
+        # alone to the other precision's step count (the autotuner's trial
+        # steps advance the members too)
+        if match_steps is not None:
+            b.close()
+            for d, n in zip(doms, match_steps):
+                left = n - d.status()["steps"]
+                while left > 0:
+                    st = d.step(left)
+                    if st["print_pending"]:
+                        d.print_done()
+                    left = n - st["steps"]
+                    if st["finished"]:
+                        break
         states = []
         for d, w in zip(doms, w0):
             st = d.status()
@@ -601,13 +615,14 @@ def run_mix(args, peak: float) -> dict:
                            "q": np.hypot(d.download("qx")[1:-1, 1:-1], d.download("qy")[1:-1, 1:-1]),
                            "steps": int(st["steps"]), "tim": st["tim"],
                            "mass_rel_err": A.water_balance(d, w)["rel_err"]})
-        b.close()
+        if match_steps is None:
+            b.close()
         for d in doms:
             d.close()
         return done / (ms / 1e3), ms, tuned, nbytes, states
 
     r32, ms32, tuned, bytes32, st32 = batch_rate("fp32")
-    r64b, ms64b, _, bytes64, st64 = batch_rate("fp64")
+    r64b, ms64b, _, bytes64, st64 = batch_rate("fp64", match_steps=[x["steps"] for x in st32])
     acc = mix_accuracy(st32, st64)
     # plain FP64 path: each scenario alone, one after another
     tot_ms, tot_cells = 0.0, 0
