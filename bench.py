@@ -555,6 +555,41 @@ def mix_accuracy(st32: list, st64: list) -> dict:
             "mass_balance_rel_fp64_max": max(b["mass_rel_err"] for b in st64)}
 
 
+def mix_envelope(scs: list, steps: list, count: int) -> dict:
+    """The scheme's own sensitivity on some of the ensemble's scenarios (the
+    smallest `count`): each runs alone in FP32, in FP64 and in two FP64 copies
+    whose initial depths are perturbed by a relative 1e-7, for the steps its
+    batch member ran; the relative L1 depth error of FP32 and of the
+    perturbed runs against FP64."""
+    from fluxos_cpp_b200 import accuracy as A
+    from fluxos_cpp_b200 import scenarios as S
+    order = sorted(range(len(scs)), key=lambda i: scs[i].nrows)[:count]
+    rows = []
+    for i in order:
+        sc, n = scs[i], steps[i]
+        runs = [S.make_domain(sc, precision="fp32", steps_in_flight=8),
+                S.make_domain(sc, precision="fp64", steps_in_flight=8)]
+        runs += [_perturbed(sc, seed, in_flight=8) for seed in (0, 1)]
+        for d in runs:
+            left = n
+            while left > 0:
+                st = d.step(left)
+                if st["print_pending"]:
+                    d.print_done()
+                left = n - st["steps"]
+                if st["finished"]:
+                    break
+        ref = runs[1]
+        e32 = A.state_errors(runs[0], ref, sc.ks)["depth"]["l1_rel"]
+        ep = [A.state_errors(d, ref, sc.ks)["depth"]["l1_rel"] for d in runs[2:]]
+        rows.append({"scenario": i, "cells": sc.nrows * sc.ncols, "steps": n, "fp32_depth_l1_rel": e32,
+                     "perturbed_fp64_depth_l1_rel": ep, "fp32_over_envelope": e32 / max(ep) if max(ep) else None})
+        for d in runs:
+            d.close()
+    return {"what": "members run alone: FP32 and two FP64 runs with initial depths perturbed by a relative "
+                    "1e-7, each against FP64, after the steps of the batch run", "members": rows}
+
+
 def run_mix(args, peak: float) -> dict:
     """The 64-scenario ensemble: FP32 batch vs FP64 batch vs FP64 one by one."""
     import torch
@@ -622,6 +657,7 @@ def run_mix(args, peak: float) -> dict:
         return done / (ms / 1e3), ms, tuned, nbytes, states
 
     r32, ms32, tuned, bytes32, st32 = batch_rate("fp32")
+    envelope = mix_envelope(scs, [x["steps"] for x in st32], args.mix_envelope_members)
     r64b, ms64b, _, bytes64, st64 = batch_rate("fp64", match_steps=[x["steps"] for x in st32])
     acc = mix_accuracy(st32, st64)
     # plain FP64 path: each scenario alone, one after another
@@ -645,7 +681,7 @@ def run_mix(args, peak: float) -> dict:
             "fp32_batch_over_fp64_batch": round(r32 / r64b, 3),
             "autotuned": {"tile_rows": tuned[0], "steps_in_flight": tuned[1]},
             "device_bytes_fp32": bytes32, "device_bytes_fp64": bytes64,
-            "host_generation_s": round(gen_s, 1), "accuracy": acc,
+            "host_generation_s": round(gen_s, 1), "accuracy": acc, "accuracy_envelope": envelope,
             "note": "per-scenario dt; timed region = one fx_batch_step of all members (CUDA events on "
                     "the batch stream); plain FP64 = each scenario alone through fx_time_steps"}
 
@@ -668,11 +704,11 @@ def front_radii(d, sc, hdry: float) -> list:
     return out
 
 
-def _perturbed(sc, seed: int):
+def _perturbed(sc, seed: int, in_flight: int = 31):
     """An FP64 domain of the scenario whose initial depths are perturbed by
     a relative 1e-7 (seeded, uniform in [-1, 1]): about one FP32 rounding."""
     from fluxos_cpp_b200 import scenarios as S
-    d = S.make_domain(sc, precision="fp64", steps_in_flight=31)
+    d = S.make_domain(sc, precision="fp64", steps_in_flight=in_flight)
     h, z = d.download("h"), d.download("z")
     dh = h * 1e-7 * np.random.default_rng(seed).uniform(-1, 1, h.shape)
     d.upload("h", h + dh)
@@ -978,6 +1014,8 @@ def main():
                     help="dam break without the two perturbed FP64 runs")
     ap.add_argument("--mix-count", type=int, default=64)
     ap.add_argument("--mix-steps", type=int, default=62)
+    ap.add_argument("--mix-envelope-members", type=int, default=4,
+                    help="ensemble scenarios also run alone in FP32, FP64 and perturbed FP64")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-c1", action="store_true", help="skip the small CPU configuration run in full")
     ap.add_argument("--no-c1-ref", action="store_true",

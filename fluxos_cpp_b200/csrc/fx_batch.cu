@@ -4,7 +4,11 @@
 // A batch of K steps is one CUDA graph: open the batch in every domain, then
 // K times (clock update of every domain, one hydrodynamic launch over the
 // concatenated tile table of all domains), then one ADE launch over the
-// interleaved unit table of all domains (fx_ade.cu). Domains that stop (an
+// interleaved unit table of all domains (fx_ade.cu). The hydrodynamic launch
+// is the persistent TMA-staged batch kernel (each domain's stencil fields
+// staged through its own tensor maps, kept in a device array) when every
+// member's grid is large enough for a staged box; otherwise one block per
+// tile loads its own stencil. Domains that stop (an
 // output is due, the run ended, or their step budget is spent) skip their
 // tiles and units until the host releases them, while the others go on.
 #include <cuda_runtime.h>
@@ -26,8 +30,12 @@ struct fx_batch {
   fx_dev* d_devs = nullptr;
   fx_tile* d_tiles = nullptr;
   fx_unit* d_units = nullptr;
-  size_t cap_devs = 0, cap_tiles = 0, cap_units = 0;
+  fx_tmaps* d_tmaps = nullptr;  // one set of tensor maps per member (batch tile shape)
+  size_t cap_devs = 0, cap_tiles = 0, cap_units = 0, cap_tmaps = 0;
   int ntiles = 0, nunits = 0, K = 1, ade_blocks = 1;
+  bool use_tma = true;   // option "tma": the TMA-staged batch kernel where the members allow it
+  bool hydro_tma = false;  // the current graph uses it
+  int tma_blocks = 0;
   int tile_rows = 8;              // hydrodynamic tile shape of the batch's launches
   int k_limit = FX_MAX_SLOTS;     // upper bound on steps per graph (ADE sweeps in flight)
   bool dirty = true;  // membership or a descriptor changed: rebuild tables and graph
@@ -103,6 +111,26 @@ static int rebuild(fx_batch* b) {
   if (!units.empty())
     FXB_CK(b, cudaMemcpyAsync(b->d_units, units.data(), sizeof(fx_unit) * units.size(), cudaMemcpyHostToDevice,
                               b->stream));
+  // tensor maps of every member for the batch's tile shape
+  b->hydro_tma = b->use_tma && n > 0;
+  for (int i = 0; i < n && b->hydro_tma; ++i)
+    if (!b->doms[i]->use_tma || !fx_tma_fits(b->doms[i], b->tile_rows)) b->hydro_tma = false;
+  if (b->hydro_tma) {
+    std::vector<fx_tmaps> tm(n);
+    for (int i = 0; i < n; ++i)
+      if ((rc = fx_build_tmaps_for(b->doms[i], b->tile_rows, &tm[i]))) {
+        b->err = fx_last_error(nullptr);
+        return rc;
+      }
+    if ((rc = grow(b, (void**)&b->d_tmaps, &b->cap_tmaps, sizeof(fx_tmaps) * n))) return rc;
+    FXB_CK(b, cudaMemcpyAsync(b->d_tmaps, tm.data(), sizeof(fx_tmaps) * n, cudaMemcpyHostToDevice, b->stream));
+    if (fx_hydro_batch_tma_blocks(b->doms[0]->d.prec32 != 0, b->tile_rows, &b->tma_blocks) != 0 ||
+        b->tma_blocks < 1) {
+      int r = fx_fail(nullptr, FX_ERR_CUDA, "occupancy query for the TMA-staged batch kernel failed");
+      b->err = fx_last_error(nullptr);
+      return r;
+    }
+  }
   FXB_CK(b, cudaStreamSynchronize(b->stream));
   b->ntiles = (int)tiles.size();
   b->nunits = (int)units.size();
@@ -125,7 +153,11 @@ static int rebuild(fx_batch* b) {
     fx_launch_batch_begin(b->d_devs, n, b->stream);
     for (int i = 0; i < b->K; ++i) {
       fx_launch_finalize(b->d_devs, n, b->stream);
-      fx_launch_hydro(b->d_devs, b->d_tiles, b->ntiles, prec32, b->tile_rows, b->stream);
+      if (b->hydro_tma)
+        fx_launch_hydro_batch_tma(b->d_devs, b->d_tmaps, b->d_tiles, b->ntiles,
+                                  std::min(b->ntiles, b->tma_blocks), prec32, b->tile_rows, b->stream);
+      else
+        fx_launch_hydro(b->d_devs, b->d_tiles, b->ntiles, prec32, b->tile_rows, b->stream);
     }
     fx_launch_ade(b->d_devs, b->d_units, b->nunits, b->ade_blocks, prec32, b->stream);
     FXB_CK(b, cudaStreamEndCapture(b->stream, &g));
@@ -164,6 +196,7 @@ void fx_batch_destroy(fx_batch* b) {
   if (b->d_devs) cudaFree(b->d_devs);
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->d_units) cudaFree(b->d_units);
+  if (b->d_tmaps) cudaFree(b->d_tmaps);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -250,6 +283,8 @@ int fx_batch_set_option(fx_batch* b, const char* name, long long v) {
   } else if (!strcmp(name, "steps_in_flight")) {
     if (v < 1 || v > FX_MAX_SLOTS - 1) return fx_fail(nullptr, FX_ERR_ARG, "steps_in_flight must be 1..63");
     b->k_limit = (int)v;
+  } else if (!strcmp(name, "tma")) {
+    b->use_tma = v != 0;
   } else {
     return fx_fail(nullptr, FX_ERR_ARG, "fx_batch_set_option: unknown option '%s'", name);
   }

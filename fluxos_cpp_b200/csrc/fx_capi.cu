@@ -160,13 +160,13 @@ static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
 // One stencil field as a 3-D tensor (irow incl. the column padding, icol,
 // plane) with a box of `box_x` x (tile_rows + 2) x 1 elements.
 static int encode_field(fx_ctx* c, fx_tmap* out, const void* base, CUtensorMapDataType type, int esz,
-                        int planes, int box_x) {
+                        int planes, int box_x, int tile_rows) {
   PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
   if (!enc) return fx_fail(c, FX_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
   const fx_dev& d = c->d;
   cuuint64_t dims[3] = {(cuuint64_t)d.ld, (cuuint64_t)(d.nc + 2), (cuuint64_t)planes};
   cuuint64_t strides[2] = {(cuuint64_t)d.ld * esz, (cuuint64_t)d.plane * esz};
-  cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)(d.tile_rows + 2), 1};
+  cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)(tile_rows + 2), 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(reinterpret_cast<CUtensorMap*>(out), type, 3, const_cast<void*>(base), dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -175,34 +175,43 @@ static int encode_field(fx_ctx* c, fx_tmap* out, const void* base, CUtensorMapDa
   return FX_OK;
 }
 
-// Tensor maps of the TMA-staged hydrodynamic kernel for the current fields
-// and tile shape (box widths: 40 4-byte, 36 8-byte, 64 1-byte elements).
-static int build_tmaps(fx_ctx* c) {
+// Tensor maps of the TMA-staged hydrodynamic kernels for the current fields
+// and a tile shape (box widths: 40 4-byte, 36 8-byte, 64 1-byte elements).
+int fx_build_tmaps_for(fx_ctx* c, int tile_rows, fx_tmaps* out) {
   const fx_dev& d = c->d;
-  fx_tmap* m = c->tmaps.m;
+  fx_tmap* m = out->m;
+  const int r = tile_rows;
   int rc;
   const CUtensorMapDataType F32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32, F64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   if (d.prec32) {
-    if ((rc = encode_field(c, &m[FX_TM_Z], d.eta, F32, 4, 2, 40)) ||
-        (rc = encode_field(c, &m[FX_TM_LO], d.eta_lo, F32, 4, 2, 40)) ||
-        (rc = encode_field(c, &m[FX_TM_QX], d.qx_f, F32, 4, 2, 40)) ||
-        (rc = encode_field(c, &m[FX_TM_QY], d.qy_f, F32, 4, 2, 40)) ||
+    if ((rc = encode_field(c, &m[FX_TM_Z], d.eta, F32, 4, 2, 40, r)) ||
+        (rc = encode_field(c, &m[FX_TM_LO], d.eta_lo, F32, 4, 2, 40, r)) ||
+        (rc = encode_field(c, &m[FX_TM_QX], d.qx_f, F32, 4, 2, 40, r)) ||
+        (rc = encode_field(c, &m[FX_TM_QY], d.qy_f, F32, 4, 2, 40, r)) ||
         (rc = encode_field(c, &m[FX_TM_MM], d.melt_mult_f ? (const void*)d.melt_mult_f : (const void*)d.eta, F32, 4,
-                           1, 40)))
+                           1, 40, r)))
       return rc;
   } else {
-    if ((rc = encode_field(c, &m[FX_TM_Z], d.z, F64, 8, 2, 36)) ||
-        (rc = encode_field(c, &m[FX_TM_LO], d.z, F64, 8, 2, 36)) ||
-        (rc = encode_field(c, &m[FX_TM_QX], d.qx, F64, 8, 2, 36)) ||
-        (rc = encode_field(c, &m[FX_TM_QY], d.qy, F64, 8, 2, 36)) ||
+    if ((rc = encode_field(c, &m[FX_TM_Z], d.z, F64, 8, 2, 36, r)) ||
+        (rc = encode_field(c, &m[FX_TM_LO], d.z, F64, 8, 2, 36, r)) ||
+        (rc = encode_field(c, &m[FX_TM_QX], d.qx, F64, 8, 2, 36, r)) ||
+        (rc = encode_field(c, &m[FX_TM_QY], d.qy, F64, 8, 2, 36, r)) ||
         (rc = encode_field(c, &m[FX_TM_MM], d.melt_mult ? (const void*)d.melt_mult : (const void*)d.z, F64, 8, 1,
-                           36)))
+                           36, r)))
       return rc;
   }
-  if ((rc = encode_field(c, &m[FX_TM_ZB], d.zb, F64, 8, 1, 36)) ||
-      (rc = encode_field(c, &m[FX_TM_FL], d.flags, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, d.nslot, 64)))
+  if ((rc = encode_field(c, &m[FX_TM_ZB], d.zb, F64, 8, 1, 36, r)) ||
+      (rc = encode_field(c, &m[FX_TM_FL], d.flags, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, d.nslot, 64, r)))
     return rc;
-  if (fx_hydro_tma_blocks(d.prec32 != 0, d.tile_rows, &c->tma_blocks) != 0 || c->tma_blocks < 1)
+  return FX_OK;
+}
+
+// The context's own maps (its tile shape) and the resident blocks of its
+// persistent launch.
+static int build_tmaps(fx_ctx* c) {
+  int rc = fx_build_tmaps_for(c, c->d.tile_rows, &c->tmaps);
+  if (rc) return rc;
+  if (fx_hydro_tma_blocks(c->d.prec32 != 0, c->d.tile_rows, &c->tma_blocks) != 0 || c->tma_blocks < 1)
     return fx_fail(c, FX_ERR_CUDA, "occupancy query for the TMA-staged hydrodynamic kernel failed");
   return FX_OK;
 }
@@ -771,7 +780,10 @@ int fx_prepare(fx_ctx* c) {
 // the ADE sweeps of all m steps in one launch (fx_ade.cu).
 // The staged kernel's boxes (64 rows of flags, tile_rows + 2 columns) must
 // fit in the field; smaller grids use the per-tile kernel.
-static bool tma_fits(const fx_ctx* c) { return c->d.ld >= 64 && c->d.nc + 2 >= c->d.tile_rows + 2; }
+// A grid at least as large as a staged box (64 rows incl. the padding, the
+// tile's columns and their halo) for a tile shape.
+bool fx_tma_fits(const fx_ctx* c, int tile_rows) { return c->d.ld >= 64 && c->d.nc + 2 >= tile_rows + 2; }
+static bool tma_fits(const fx_ctx* c) { return fx_tma_fits(c, c->d.tile_rows); }
 
 static void launch_hydro(fx_ctx* c) {
   if (c->use_tma && tma_fits(c)) fx_launch_hydro_tma(c->d, c->tmaps, c->tma_blocks, c->stream);

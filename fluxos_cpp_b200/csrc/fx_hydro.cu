@@ -1715,6 +1715,133 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
   reduce_part(d, S, acc);
 }
 
+// ---- TMA-staged persistent form for a batch --------------------------------
+// Each block walks a contiguous range of the packed tile table of all the
+// batch's domains (so it crosses few domain boundaries). Thread 0 stages the
+// stencil of the block's next tile with that domain's own tensor maps (a
+// device array, one set per domain) while the block computes the current
+// tile; a domain without a solver step this launch (stopped, or no wet cell)
+// gets no stage. The domain's descriptor and step fields sit in shared
+// memory while the block works on its tiles, and the block's Courant and
+// budget partials go to a domain when the block leaves it.
+
+// Thread 0: stage tile t of the table into `stg` if its domain runs the
+// solver this step; returns whether a copy was issued.
+template <bool P32, int BY>
+__device__ __forceinline__ bool batch_stage(const fx_dev* __restrict__ devs, const fx_tmaps* __restrict__ tms,
+                                            const fx_tile* __restrict__ tiles, int t, unsigned char* stg,
+                                            unsigned long long* bar, int& fenced) {
+  const fx_tile tl = tiles[t];
+  const fx_dev& dm = devs[tl.dom];
+  const fx_ctl& g = *dm.ctl;
+  if (!g.live || !g.active) return false;
+  const fx_tmaps& tm = tms[tl.dom];
+  if (fenced != tl.dom) {
+    // the maps were written by a host copy before the launch; order the
+    // tensor-map proxy's reads of a domain's maps after it, once per domain
+    for (int f = 0; f < FX_TM_COUNT; ++f)
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&tm.m[f]) : "memory");
+    fenced = tl.dom;
+  }
+  const int ntx = (dm.nr + TX - 1) / TX;
+  stage_issue<P32, BY>(dm, tm, tl.by * ntx + tl.bx, ntx, g.steps - 1, stg, bar);
+  return true;
+}
+
+template <bool P32, int BY>
+__global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
+    k_hydro_batch_tma(const fx_dev* __restrict__ devs, const fx_tmaps* __restrict__ tms,
+                      const fx_tile* __restrict__ tiles, int ntiles) {
+  using L = StageLayout<P32, BY>;
+  __shared__ HydroSmem<BY> S;
+  __shared__ fx_dev sd;
+  __shared__ StepCtl sc;
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ int staged[2];  // the tile each stage holds (-1: none)
+  __shared__ int abort_flag;
+  extern __shared__ __align__(128) unsigned char dyn[];
+  unsigned char* stage0 = dyn + ((128 - (smem_u32(dyn) & 127)) & 127);
+  const int tid = threadIdx.y * BX + threadIdx.x;
+  const int t0 = (int)((long long)ntiles * blockIdx.x / gridDim.x);
+  const int t1 = (int)((long long)ntiles * (blockIdx.x + 1) / gridDim.x);
+  if (t0 >= t1) return;
+  int fenced = -1;  // thread 0: the domain whose maps it last fenced
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+    staged[0] = batch_stage<P32, BY>(devs, tms, tiles, t0, stage0, &bar[0], fenced) ? t0 : -1;
+    staged[1] = -1;
+  }
+  __syncthreads();
+  unsigned parity = 0u;  // bit q: phase of stage q's barrier
+  int st = 0, dom = -1;
+  TilePart acc = tile_part();
+  for (int t = t0; t < t1; ++t) {
+    const fx_tile tl = tiles[t];
+    if (tl.dom != dom) {
+      if (dom >= 0) reduce_part(sd, S, acc);  // the partials of the domain the block leaves
+      acc = tile_part();
+      __syncthreads();
+      const unsigned long long* src = reinterpret_cast<const unsigned long long*>(devs + tl.dom);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+      for (int i = tid; i < (int)(sizeof(fx_dev) / 8); i += BX * BY) dst[i] = src[i];
+      __syncthreads();
+      if (tid == 0) {
+        const fx_ctl& g = *sd.ctl;
+        sc.dtfl = g.dtfl;
+        sc.meteoi = g.meteoi;
+        sc.meteo_rate = g.meteo_rate;
+        sc.mconc = g.mconc;
+        sc.inflowi = g.inflowi;
+        sc.twet_inc = g.dtfl / 3600;
+        sc.steps = g.steps;
+        sc.live = g.live;
+        sc.active = g.active;
+      }
+      __syncthreads();
+      dom = tl.dom;
+    }
+    if (tid == 0)
+      staged[st ^ 1] = (t + 1 < t1 && batch_stage<P32, BY>(devs, tms, tiles, t + 1, stage0 + (st ^ 1) * L::BYTES,
+                                                           &bar[st ^ 1], fenced))
+                           ? t + 1 : -1;
+    const bool mine = staged[st] == t;  // this tile's stencil is (being) staged
+    if (mine) {
+      long long it = 0;
+      while (!mbar_try_wait(&bar[st], (parity >> st) & 1u)) {
+        if (++it > STAGE_SPIN_LIMIT) {
+          abort_flag = 1;
+          break;
+        }
+      }
+      parity ^= 1u << st;
+    }
+    __syncthreads();
+    if (abort_flag) {
+      if (tid == 0) {
+        atomicCAS(&sd.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
+        long long w = 0;  // let a copy already issued for the next tile land before the block exits
+        if (staged[st ^ 1] >= 0)
+          while (!mbar_try_wait(&bar[st ^ 1], (parity >> (st ^ 1)) & 1u) && ++w < STAGE_SPIN_LIMIT) {
+          }
+      }
+      return;
+    }
+    const StepCtl c = sc;
+    if (c.live) {
+      const fx_tile tile{0, tl.bx, tl.by, 0};
+      const unsigned char* stg = mine ? stage0 + st * L::BYTES : nullptr;
+      if constexpr (P32) hydro_tile32<BY>(sd, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S), acc, stg);
+      else hydro_tile64<BY>(sd, c, tile, S, acc, stg);
+    }
+    __syncthreads();  // the stage is free for the copy issued next iteration
+    st ^= 1;
+  }
+  if (dom >= 0) reduce_part(sd, S, acc);
+}
+
 // Courant scan of the state as uploaded (the scan at the top of the first
 // step). Also used after a host edit of the state.
 template <int BY>
@@ -1949,6 +2076,50 @@ int tma_blocks(int* out) {
   return 0;
 }
 }  // namespace
+
+namespace {
+template <bool P32, int BY>
+size_t batch_tma_dyn() { return (size_t)2 * fx::StageLayout<P32, BY>::BYTES + 128; }
+template <int BY>
+void launch_hydro_batch_tma(const fx_dev* devs, const fx_tmaps* tms, const fx_tile* tiles, int ntiles, int nblocks,
+                            bool prec32, cudaStream_t s) {
+  if (prec32)
+    fx::k_hydro_batch_tma<true, BY><<<nblocks, dim3(fx::BX, BY), batch_tma_dyn<true, BY>(), s>>>(devs, tms, tiles,
+                                                                                              ntiles);
+  else
+    fx::k_hydro_batch_tma<false, BY><<<nblocks, dim3(fx::BX, BY), batch_tma_dyn<false, BY>(), s>>>(devs, tms, tiles,
+                                                                                                ntiles);
+}
+template <bool P32, int BY>
+int batch_tma_blocks(int* out) {
+  const size_t dyn = batch_tma_dyn<P32, BY>();
+  if (cudaFuncSetAttribute(fx::k_hydro_batch_tma<P32, BY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) !=
+      cudaSuccess)
+    return -1;
+  int dev = 0, nsm = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fx::k_hydro_batch_tma<P32, BY>, fx::BX * BY, dyn) !=
+      cudaSuccess)
+    return -1;
+  *out = per * nsm;
+  return 0;
+}
+}  // namespace
+
+// The TMA-staged persistent hydrodynamic launch of a batch: `tms` holds one
+// set of tensor maps per domain, built for `tile_rows`.
+void fx_launch_hydro_batch_tma(const fx_dev* devs, const fx_tmaps* tms, const fx_tile* tiles, int ntiles,
+                               int nblocks, bool prec32, int tile_rows, cudaStream_t s) {
+  if (tile_rows == 4) launch_hydro_batch_tma<4>(devs, tms, tiles, ntiles, nblocks, prec32, s);
+  else if (tile_rows == 16) launch_hydro_batch_tma<16>(devs, tms, tiles, ntiles, nblocks, prec32, s);
+  else launch_hydro_batch_tma<8>(devs, tms, tiles, ntiles, nblocks, prec32, s);
+}
+int fx_hydro_batch_tma_blocks(bool prec32, int tile_rows, int* out) {
+  if (tile_rows == 4) return prec32 ? batch_tma_blocks<true, 4>(out) : batch_tma_blocks<false, 4>(out);
+  if (tile_rows == 16) return prec32 ? batch_tma_blocks<true, 16>(out) : batch_tma_blocks<false, 16>(out);
+  return prec32 ? batch_tma_blocks<true, 8>(out) : batch_tma_blocks<false, 8>(out);
+}
 
 void fx_launch_hydro_tma(const fx_dev& d, const fx_tmaps& tm, int nblocks, cudaStream_t s) {
   if (d.tile_rows == 4) launch_hydro_tma<4>(d, tm, nblocks, s);

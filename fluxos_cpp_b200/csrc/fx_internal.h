@@ -70,6 +70,12 @@ void fx_launch_hydro(const fx_dev* devs, const fx_tile* tiles, int ntiles, bool 
 void fx_launch_hydro_one(const fx_dev& d, cudaStream_t s);
 void fx_launch_hydro_tma(const fx_dev& d, const fx_tmaps& tm, int nblocks, cudaStream_t s);
 int fx_hydro_tma_blocks(bool prec32, int tile_rows, int* out);
+void fx_launch_hydro_batch_tma(const fx_dev* devs, const fx_tmaps* tms, const fx_tile* tiles, int ntiles,
+                               int nblocks, bool prec32, int tile_rows, cudaStream_t s);
+int fx_hydro_batch_tma_blocks(bool prec32, int tile_rows, int* out);
+// Tensor maps of a context's stencil fields for a tile shape (fx_capi.cu).
+int fx_build_tmaps_for(fx_ctx* c, int tile_rows, fx_tmaps* out);
+bool fx_tma_fits(const fx_ctx* c, int tile_rows);
 void fx_launch_courant_scan(const fx_dev* devs, const fx_tile* tiles, int ntiles, int tile_rows, cudaStream_t s);
 void fx_launch_ade(const fx_dev* devs, const fx_unit* units, int nunits, int nblocks, bool prec32, cudaStream_t s);
 void fx_launch_ade_one(const fx_dev& d, int nunits, int nblocks, cudaStream_t s);

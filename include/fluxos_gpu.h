@@ -198,8 +198,10 @@ int fx_batch_size(const fx_batch* b);
 int fx_batch_step(fx_batch* b, int nsteps, fx_status* st);
 void* fx_batch_stream(fx_batch* b);
 /* Options of the batch's launches: "tile_rows" (4, 8, 16, as for
- * fx_set_option) and "steps_in_flight" (upper bound on the steps per graph,
- * 1..63; the members' own steps_in_flight bound it too). */
+ * fx_set_option), "steps_in_flight" (upper bound on the steps per graph,
+ * 1..63; the members' own steps_in_flight bound it too) and "tma" (1, the
+ * default: the persistent TMA-staged hydrodynamic kernel when every member
+ * allows it; 0: one block per tile; results are identical). */
 int fx_batch_set_option(fx_batch* b, const char* name, long long value);
 /* Autotuner of the batch: tries each tile shape, then each steps-in-flight
  * bound (2, 4, 8, 16, 31, 63, up to the members' own), for trial_steps real

@@ -134,3 +134,39 @@ def test_batch_autotuner_keeps_results():
         for key in ("z", "h", "qx", "conc"):
             assert np.array_equal(m.download(key), solo.download(key)), key
     b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_staged_kernel_matches_per_tile_kernel_and_alone(precision):
+    """The persistent TMA-staged batch kernel (blocks walking ranges of the
+    packed tile table, each domain staged through its own tensor maps) and
+    the one-block-per-tile batch kernel give identical states, equal to each
+    domain stepped alone; one member is dry (no solver step, so no stage)
+    while the others are wet."""
+    scs = [_fractal_wet(n, 40 + i) for i, n in enumerate((61, 150, 96))]
+    dry = S.plane_scenario(64, 70, seed=9)
+    dry.horizon, dry.meteo = 1e5, ((0.0, 0.0, 0.0), (1e5, 0.0, 0.0))  # stays dry
+    scs.append(dry)
+    keys = ("z", "h", "qx", "qy", "conc", "fe_1", "fn_1", "twet")
+    out = {}
+    for tma in (1, 0):
+        b = fx.Batch()
+        b.set_option("tma", tma)
+        b.set_option("tile_rows", 8)
+        ms = [S.make_domain(sc, precision=precision, steps_in_flight=8) for sc in scs]
+        for m in ms:
+            b.add(m)
+        _run_batch(b, 25)
+        out[tma] = [{k: m.download(k) for k in keys} for m in ms]
+        out[f"st{tma}"] = [m.status() for m in ms]
+        b.close()
+        for m in ms:
+            m.close()
+    assert out["st1"][-1]["hpall"] == 0  # the dry member has not run the solver
+    for i, sc in enumerate(scs):
+        solo = S.make_domain(sc, precision=precision, steps_in_flight=8)
+        GP.advance_domain(solo, out["st1"][i]["steps"])
+        for k in keys:
+            assert np.array_equal(out[1][i][k], out[0][i][k]), (i, k)
+            assert np.array_equal(out[1][i][k], solo.download(k)), (i, k)
+        solo.close()
