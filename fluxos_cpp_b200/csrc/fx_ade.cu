@@ -46,7 +46,8 @@ namespace fxade {
 
 constexpr int ROWS = 30;      // rows per strip (lanes 0..29 compute)
 constexpr int WARPS = 4;      // warps per block
-constexpr int CHUNK = 8;      // steps between progress checks and publications
+constexpr int CHUNK = 4;      // steps between progress checks and publications (the lag between
+                              // strips is 2 * CHUNK + ROWS - 1 warp steps)
 constexpr int RING = 4;       // per-lane prefetch slots (a power of two); a deeper ring takes shared
                               // memory from L1, which the lanes' skewed reads depend on (measured:
                               // 8 slots made the FP64 sweep 2.5x slower)
@@ -198,12 +199,11 @@ __device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const
   cp_async4(&R.fl[slot][lane], d.flags + S.cur + (gi & ~3LL), inr);
 }
 
-// The record of cell (ix, iy) from its ring slot: add_meteo's dilution
-// (common.cpp:214-234) when the step has one, then the re-scale of
-// ADEsolver_calc.cpp:64-72 when the step sweeps. Ghost cells carry only their
-// depth (their concentration is 0 and never changes).
+// The same record with the tests as branches (the FP64 state: lanes skip the
+// IEEE divisions their cell does not need, which in FP64 costs more than the
+// divergence).
 template <class T>
-__device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, const Ring<T>& R, int lane, int ix,
+__device__ __forceinline__ Rec<T> make_rec_br(const fx_dev& d, const StepIn& S, const Ring<T>& R, int lane, int ix,
                                            int iy) {
   Rec<T> r;
   r.c = T(0);
@@ -251,6 +251,65 @@ __device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, con
   return r;
 }
 
+// The record of cell (ix, iy) from its ring slot: add_meteo's dilution
+// (common.cpp:214-234) when the step has one, then the re-scale of
+// ADEsolver_calc.cpp:64-72 when the step sweeps. Ghost cells carry only their
+// depth (their concentration is 0 and never changes). The slot is always a
+// ring entry, so it is read for every (ix, iy) and the values are selected:
+// per-cell tests become selects and the block has no divergent branch (the
+// step's dilution and point inflow are the same for the whole warp). Used by
+// the FP32 state, whose divisions are a few fused operations.
+template <class T>
+__device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, const Ring<T>& R, int lane, int ix,
+                                           int iy) {
+  const bool inr = ix >= 0 && ix <= d.nr + 1 && iy >= 0 && iy <= d.nc + 1;
+  const bool interior = ix >= 1 && ix <= d.nr && iy >= 1 && iy <= d.nc;
+  const int slot = iy & (RING - 1);
+  const long long gi = fx_ix(d, ix, iy);  // an index into the ring's groups only, outside the grid
+  const unsigned fl = (R.fl[slot][lane] >> (8 * (unsigned)(gi & 3))) & 0xffu;
+  const int ld = fl & FX_F_LDRY;
+  const bool ldp = (fl & FX_F_LDRY_PREV) != 0;
+  const T h = R.h[slot][lane];
+  const T h0 = R.h0[slot][lane];
+  T c = R.c[slot][lane][gi & (Ring<T>::CV - 1)];
+  // the inflow cell holds h0 only after its inflow; the melt's dilution
+  // divides by the depth after the melt (common.cpp:226-234, 313-325)
+  const bool inflow_cell = S.inflow_gi >= 0 && interior && gi == S.inflow_gi;
+  const T hm = inflow_cell ? (T)S.inflow_hm : h0;
+  if (S.dilute) {
+    const T hp = R.hp[slot][lane];
+    // the melt depth the hydrodynamic step added (FP32 state: melt32 in fx_hydro.cu)
+    T mi;
+    if constexpr (sizeof(T) == 4)
+      mi = Fields<T>::mm(d) ? (T)(S.meteoi * (double)R.mm[slot][lane]) : (T)S.meteoi;
+    else
+      mi = Fields<T>::mm(d) ? (T)((double)S.meteo_rate * (double)R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
+                            : (T)S.meteoi;
+    const bool use = !(fl & FX_F_NODATA) && hp != T(0);  // then hm >= hp > 0
+    const T cd = tdiv(c * hp + (mi * (T)S.mconc), use ? hm : T(1));
+    c = use ? cd : c;
+  }
+  if (S.inflow_gi >= 0) {
+    const bool use = inflow_cell && hm != T(0);
+    const T ci = tdiv(c * hm + (T)(S.inflowi * S.iconc), use ? h0 : T(1));
+    c = use ? ci : c;
+  }
+  T b = c;
+  if (S.sweep) {
+    const bool wet2 = ld == 0 && !ldp;  // wet before and after the step: h > hdry
+    const T bw = tdiv(c * h0, wet2 ? h : T(1));
+    b = wet2 ? bw : (ld == 1 ? T(0) : c);
+  }
+  Rec<T> r;
+  r.h = inr ? h : T(0);
+  r.c = interior ? c : T(0);
+  r.b = interior ? b : T(0);
+  r.qx = interior ? R.fe1[slot][lane] : T(0);
+  r.qy = interior ? R.fn1[slot][lane] : T(0);
+  r.ld = interior ? ld : 0;
+  return r;
+}
+
 template <class V>
 __device__ __forceinline__ V shfl_d(V v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 template <class V>
@@ -258,9 +317,9 @@ __device__ __forceinline__ V shdn(V v, int k) { return __shfl_down_sync(0xffffff
 template <class V>
 __device__ __forceinline__ V shup(V v, int k) { return __shfl_up_sync(0xffffffffu, v, k); }
 
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
   unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
@@ -272,6 +331,86 @@ __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long 
 // state's (same operations, same order).
 template <class T>
 __device__ __forceinline__ void ade_cell(const fx_dev& d, T D, T dt, bool last_row, bool last_col, T hp,
+                                         T he, T hn, T qxl, T qyl, T fw, T fp, T fe, T fee, T fs, T fn,
+                                         T fnn, T pfw, T qfs, int ldE, int ldW, int ldEE, int ldN, int ldS,
+                                         int ldNN, T cmax, T cmin, T& con, T& pfe_out, T& qfn_out) {
+  // The expressions of ADEsolver_calc.cpp:126-288 in the same order and
+  // operand types; both sides of every test are evaluated and the result
+  // selected, so the cell is one straight-line block (independent parts of
+  // the E and N faces interleave). A quotient that is not selected divides by
+  // 1 instead of a possibly zero denominator (an FP64 division by zero takes
+  // the division's slow path); a selected one is unchanged.
+  const T nt = 1;
+  const T dx = (T)d.dxy, dy = (T)d.dxy;
+  const T area = (T)d.arbase, areae = (T)d.arbase, arean = (T)d.arbase;
+  const T ntp = nt;
+  const bool wetE = ldE == 0, wetN = ldN == 0;
+  // E face (:151-194)
+  const T hnue_e = fmax(hp * nt * he * nt, T(.0001));
+  const T hne = div_dxy<T>(d, tsqrt(hnue_e) * T(2)) * dy * D;  // sigc = 0.5: /sigc is *2 exactly
+  const T pfde = wetE ? -hne * (fe - fp) : T(0);
+  const T mid_e = T(.5) * fp + T(.5) * fe;
+  const T up_e = ldW == 0 ? T(-.125) * fw + T(.75) * fp + T(.375) * fe : mid_e;
+  const T dn_e = ldEE == 0 ? T(.375) * fp + T(.75) * fe - T(.125) * fee : mid_e;
+  T fem = wetE ? (qxl > T(0) ? up_e : dn_e) : T(0);
+  fem = fmax(T(0), fem);
+  fem = last_row ? T(0) : fem;  // :176-178, ghost concentration c(NROWS+1, iy) = 0
+  const T pfce = qxl * fem * dy;
+  T pfe = pfce + pfde;
+  const T cvolrate_e = tdiv(-(fe * he) * areae, dt);
+  pfe = pfe < T(0) ? (wetE ? fmax(pfe, cvolrate_e) : T(0)) : pfe;
+  // N face (:198-241)
+  const T hnue_n = fmax(T(.0001), hp * ntp * hn * nt);
+  const T hnn = div_dxy<T>(d, tsqrt(hnue_n) * T(2)) * dx * D;
+  const T qfdn = wetN ? -hnn * (fn - fp) : T(0);
+  const T mid_n = T(.5) * fp + T(.5) * fn;
+  const T up_n = ldS == 0 ? T(-.125) * fs + T(.75) * fp + T(.375) * fn : mid_n;
+  const T dn_n = ldNN == 0 ? T(.375) * fp + T(.75) * fn - T(.125) * fnn : mid_n;
+  T fnm = wetN ? (qyl > T(0) ? up_n : dn_n) : T(0);
+  fnm = fmax(T(0), fnm);
+  fnm = last_col ? T(0) : fnm;  // :223-225, ghost concentration c(ix, NCOLS+1) = 0
+  const T qfcn = qyl * fnm * dx;
+  T qfn = qfcn + qfdn;
+  const T cvolrate_n = tdiv(-(fn * hn) * arean, dt);
+  qfn = qfn < T(0) ? (wetN ? fmax(qfn, cvolrate_n) : T(0)) : qfn;
+  // outflow limiter (:243-278)
+  const T cvolpot = (fp * hp) * area;
+  const T cvolrat = tdiv(cvolpot, dt) + pfw + qfs;
+  const T sum = pfe + qfn;
+  const bool pos = cvolrat > T(0);
+  const bool pp = pfe > T(0), qp = qfn > T(0);
+  // cvolrat > 0
+  const bool both = pp && qp;
+  const bool split = both && sum > cvolrat;
+  const T cf = tdiv(qfn, split ? sum : T(1));
+  T pfe_a = split ? (T(1) - cf) * cvolrat : pfe;
+  T qfn_a = split ? cf * cvolrat : qfn;
+  pfe_a = (!both && pp) ? fmin(pfe, (cvolrat - qfn)) : pfe_a;
+  qfn_a = (!both && !pp && qp) ? fmin(qfn, (cvolrat - pfe)) : qfn_a;
+  // cvolrat <= 0
+  const bool c1 = pfe >= T(0) && qfn < T(0);
+  const bool c2 = !c1 && pfe < T(0) && qfn >= T(0);
+  const bool c3 = !c1 && !c2 && pfe >= T(0) && qfn >= T(0);
+  const T cb1 = cvolrat - qfn, cb2 = cvolrat - pfe;
+  T pfe_b = c1 ? (cb1 > T(0) ? fmin(pfe, cb1) : T(0)) : pfe;
+  T qfn_b = c2 ? (cb2 > T(0) ? fmin(qfn, cb2) : T(0)) : qfn;
+  pfe_b = c3 ? T(0) : pfe_b;
+  qfn_b = c3 ? T(0) : qfn_b;
+  pfe = pos ? pfe_a : pfe_b;
+  qfn = pos ? qfn_a : qfn_b;
+  const T dc = div_area<T>(d, (pfw - pfe + qfs - qfn) * dt);  // :281-286
+  T cn = fp + tdiv(dc, hp != T(0) ? hp : T(1));  // hp is 0 only in a dry cell, whose result is not kept
+  cn = fmin(cmax, cn);
+  cn = fmax(cmin, cn);
+  con = cn;
+  pfe_out = pfe;
+  qfn_out = qfn;
+}
+
+// The same cell with the tests as branches (the FP64 state, for the reason
+// given at make_rec_br).
+template <class T>
+__device__ __forceinline__ void ade_cell_br(const fx_dev& d, T D, T dt, bool last_row, bool last_col, T hp,
                                          T he, T hn, T qxl, T qyl, T fw, T fp, T fe, T fee, T fs, T fn,
                                          T fnn, T pfw, T qfs, int ldE, int ldW, int ldEE, int ldN, int ldS,
                                          int ldNN, T cmax, T cmin, T& con, T& pfe_out, T& qfn_out) {
@@ -423,15 +562,19 @@ __device__ __forceinline__ bool wait_deps(const fx_dev& d, Deps& D, int need_w, 
     const bool ok = dep_ok(D.w, D.seen_w, D.tag_w, need_w) && dep_ok(D.p0, D.seen_p0, D.tag_p, need_p0) &&
                     dep_ok(D.p1, D.seen_p1, D.tag_p, need_p1) && (!hold || (!D.w && !D.p0 && !D.p1));
     if (__all_sync(0xffffffffu, ok)) return true;
-    const bool stop = (++it > limit) || (*(volatile int*)&d.ctl->error != 0);
+    const bool stop = (++it > limit) || ((it & 63) == 0 && *(volatile int*)&d.ctl->error != 0);
     if (__any_sync(0xffffffffu, stop)) {
       if ((threadIdx.x & 31) == 0) atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
       return false;
     }
     if (it > 1) __nanosleep(it < 8 ? 64 : (it < 64 ? 256 : 1024));
-    const unsigned long long a = D.w ? ld_acquire(D.w) : 0ull;
-    const unsigned long long b = D.p0 ? ld_acquire(D.p0) : 0ull;
-    const unsigned long long c = D.p1 ? ld_acquire(D.p1) : 0ull;
+    // the three counters in one round trip (relaxed loads in flight
+    // together), then one fence: with the producers' release stores it orders
+    // this warp's later reads of their data after the counts it saw
+    const unsigned long long a = D.w ? ld_relaxed(D.w) : 0ull;
+    const unsigned long long b = D.p0 ? ld_relaxed(D.p0) : 0ull;
+    const unsigned long long c = D.p1 ? ld_relaxed(D.p1) : 0ull;
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     D.seen_w = a;
     D.seen_p0 = b;
     D.seen_p1 = c;
@@ -518,9 +661,13 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
       }
     }
     cp_wait<0>();
-    Rec<T> cur = make_rec<T>(d, S, R, lane, ix, iy0);
-    Rec<T> n1 = make_rec<T>(d, S, R, lane, ix, iy0 + 1);
-    Rec<T> n2 = make_rec<T>(d, S, R, lane, ix, iy0 + 2);
+    auto rec_at = [&](int col) {
+      if constexpr (sizeof(T) == 4) return make_rec<T>(d, S, R, lane, ix, col);
+      else return make_rec_br<T>(d, S, R, lane, ix, col);
+    };
+    Rec<T> cur = rec_at(iy0);
+    Rec<T> n1 = rec_at(iy0 + 1);
+    Rec<T> n2 = rec_at(iy0 + 2);
     if (!bail) {
       for (int j = 3; j < DIST + 3; ++j) {
         prefetch<T>(d, S, A, R, lane, ix, iy0 + j);
@@ -574,10 +721,16 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
         }
       }
       const int iy = tau - lane + 1;
-      // keep DIST columns in flight: column iy + DIST + 3 now, column iy + 3
-      // must have landed by the end of this step
+      // keep DIST columns in flight: column iy + DIST + 3 now; column iy + 3,
+      // copied DIST steps ago, has landed after cp_wait and becomes the record
+      // of the next step, made here so that its arithmetic and this step's
+      // cell interleave
       prefetch<T>(d, S, A, R, lane, ix, iy + DIST + 3);
       cp_commit();
+      cp_wait<DIST>();
+      Rec<T> n3;
+      if constexpr (sizeof(T) == 4) n3 = make_rec<T>(d, S, R, lane, ix, iy + 3);
+      else n3 = make_rec_br<T>(d, S, R, lane, ix, iy + 3);
       // east (lane+1's next column), east-east (lane+2's column after next)
       const T E_c = shdn(n1.c, 1), E_b = shdn(n1.b, 1), E_h = shdn(n1.h, 1);
       const int E_ld = __shfl_down_sync(0xffffffffu, n1.ld, 1);
@@ -607,16 +760,32 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
         }
         const T NN_b = last_col ? n1.b : n2.b;  // inn = min(iy+2, NCOLS+1)
         const int NN_ld = last_col ? n1.ld : n2.ld;
-        if (!S.sweep || (last_row && last_col)) {
+        if constexpr (sizeof(T) == 4) {
+          // the cell is computed for every lane and kept only for a wet cell
+          // the sweep reaches: a dry cell gets 0 and no fluxes (:119-124), a
+          // step without a sweep and the cell the sweep stops short of (:93)
+          // keep the re-scaled value
+          const T cmax = fmax(W_b, fmax(E_c, fmax(o_b, n1.c)));
+          const T cmin = fmin(W_b, fmin(E_c, fmin(o_b, n1.c)));
+          T cell_c, cell_pfe, cell_qfn;
+          ade_cell<T>(d, D, (T)S.dt, last_row, last_col, cur.h, E_h, n1.h, cur.qx, cur.qy, W_c, cur.b, E_b,
+                   EE_b, o_c, n1.b, NN_b, W_pfe, o_qfn, E_ld, W_ld, EE_ld, n1.ld, o_ld, NN_ld, cmax,
+                   cmin, cell_c, cell_pfe, cell_qfn);
+          const bool keep = !S.sweep || (last_row && last_col);
+          const bool swept = !keep && cur.ld != 1;
+          out_c = keep ? cur.b : (swept ? cell_c : T(0));
+          pfe = swept ? cell_pfe : T(0);
+          qfn = swept ? cell_qfn : T(0);
+        } else if (!S.sweep || (last_row && last_col)) {
           out_c = cur.b;  // no sweep this step, or the cell the sweep stops short of (:93)
         } else if (cur.ld == 1) {
           out_c = T(0);  // :119-124
         } else {
           const T cmax = fmax(W_b, fmax(E_c, fmax(o_b, n1.c)));
           const T cmin = fmin(W_b, fmin(E_c, fmin(o_b, n1.c)));
-          ade_cell<T>(d, D, (T)S.dt, last_row, last_col, cur.h, E_h, n1.h, cur.qx, cur.qy, W_c, cur.b, E_b,
-                   EE_b, o_c, n1.b, NN_b, W_pfe, o_qfn, E_ld, W_ld, EE_ld, n1.ld, o_ld, NN_ld, cmax,
-                   cmin, out_c, pfe, qfn);
+          ade_cell_br<T>(d, D, (T)S.dt, last_row, last_col, cur.h, E_h, n1.h, cur.qx, cur.qy, W_c, cur.b, E_b,
+                      EE_b, o_c, n1.b, NN_b, W_pfe, o_qfn, E_ld, W_ld, EE_ld, n1.ld, o_ld, NN_ld, cmax,
+                      cmin, out_c, pfe, qfn);
         }
         // the sweep's neighbours and the next strip read the value before the
         // soil release, which follows the whole sweep in the reference
@@ -641,19 +810,20 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
         o_qfn = T(0);
       }
       // publish progress: every lane's writes of this chunk, then the count.
-      // The next strip of this step overwrites its first two rows only after
-      // this count passes the column by ROWS steps; lanes 30 and 31 copied
-      // those rows DIST + 3 columns ahead, and cp_wait below retires a copy
-      // DIST steps after it was issued, so the copies have landed by then.
+      // The warp barrier orders the other lanes' writes before lane 0's
+      // release store, which makes them visible with the count to a warp
+      // that reads it and then fences. The next strip of this step overwrites
+      // its first two rows only after this count passes the column by ROWS
+      // steps; lanes 30 and 31 copied those rows DIST + 3 columns ahead, and
+      // cp_wait retires a copy DIST steps after it was issued, so the copies
+      // have landed by then.
       if (((tau + 1) % CHUNK) == 0 || tau + 1 == TW) {
-        __threadfence();
         __syncwarp();
         if (lane == 0) st_release(prog_me, (tag << 32) | (unsigned)(tau + 1));
       }
-      cp_wait<DIST>();
       cur = n1;
       n1 = n2;
-      n2 = make_rec<T>(d, S, R, lane, ix, iy + 3);
+      n2 = n3;
     }
     cp_wait<0>();
     return !bail;
