@@ -561,23 +561,24 @@ __device__ __forceinline__ bool wait_deps(const fx_dev& d, Deps& D, int need_w, 
   for (;;) {
     const bool ok = dep_ok(D.w, D.seen_w, D.tag_w, need_w) && dep_ok(D.p0, D.seen_p0, D.tag_p, need_p0) &&
                     dep_ok(D.p1, D.seen_p1, D.tag_p, need_p1) && (!hold || (!D.w && !D.p0 && !D.p1));
-    if (__all_sync(0xffffffffu, ok)) return true;
+    if (__all_sync(0xffffffffu, ok)) {
+      // the counts that sufficed were read by relaxed loads: one fence orders
+      // this warp's later reads of the producers' data after them (with the
+      // producers' release stores). Counts kept from an earlier wait were
+      // followed by this fence then.
+      if (it > 0) asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      return true;
+    }
     const bool stop = (++it > limit) || ((it & 63) == 0 && *(volatile int*)&d.ctl->error != 0);
     if (__any_sync(0xffffffffu, stop)) {
       if ((threadIdx.x & 31) == 0) atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
       return false;
     }
     if (it > 1) __nanosleep(it < 8 ? 64 : (it < 64 ? 256 : 1024));
-    // the three counters in one round trip (relaxed loads in flight
-    // together), then one fence: with the producers' release stores it orders
-    // this warp's later reads of their data after the counts it saw
-    const unsigned long long a = D.w ? ld_relaxed(D.w) : 0ull;
-    const unsigned long long b = D.p0 ? ld_relaxed(D.p0) : 0ull;
-    const unsigned long long c = D.p1 ? ld_relaxed(D.p1) : 0ull;
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");
-    D.seen_w = a;
-    D.seen_p0 = b;
-    D.seen_p1 = c;
+    // the three counters in one round trip (relaxed loads in flight together)
+    D.seen_w = D.w ? ld_relaxed(D.w) : 0ull;
+    D.seen_p0 = D.p0 ? ld_relaxed(D.p0) : 0ull;
+    D.seen_p1 = D.p1 ? ld_relaxed(D.p1) : 0ull;
   }
 }
 
