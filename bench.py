@@ -79,10 +79,11 @@ ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
 # DRAM bytes per cell that each kernel actually moves per step
 # (dram__bytes_read.sum + dram__bytes_write.sum from ncu on the 2048 x 2048
 # case of this workload, one launch, divided by the cells and the steps the
-# launch covers); traffic scales with the cells, so `traffic` in the line is
-# this times the cells of the run.
-DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 143.59, "k_ade_sweep": 61.35},
-                       "fp32": {"k_hydro": 80.38, "k_ade_sweep": 26.65}}
+# launch covers: profiles/k_ade_one_fractal2048.md,
+# profiles/k_hydro_tma_fractal2048.md); traffic scales with the cells, so
+# `traffic` in the line is this times the cells of the run.
+DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 143.32, "k_ade_sweep": 49.33},
+                       "fp32": {"k_hydro": 80.45, "k_ade_sweep": 23.66}}
 
 
 def _rank():
