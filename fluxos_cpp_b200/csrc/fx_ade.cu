@@ -643,11 +643,19 @@ __device__ __forceinline__ bool ade_unit(const fx_dev& d, Ring<T>& R, int jj, in
     dep.tag_w = tag;
     dep.tag_p = tag - 1;
     dep.seen_w = dep.seen_p0 = dep.seen_p1 = 0ull;
-    // the previous step must have written every column prefetched before a
-    // check (lanes 0..29 of its strip s, lanes 0..1 of its strip s + 1), and
-    // the west strip of this step the boundary columns read in the chunk
-    auto need_p0 = [&](int col) { return min(col + ROWS, TW); };
-    auto need_p1 = [&](int col) { return min(col + 2, TW); };
+    // the previous step must have written every cell prefetched before the
+    // next check, and the west strip of this step the boundary columns read
+    // in the chunk. When lane 0 prefetches up to column col, lane t (< ROWS)
+    // prefetches its row up to column col - t, which lane t of the previous
+    // step's sweep of this strip, on the same skew, updates at warp step
+    // col - 1: a count of col suffices. Lanes ROWS and ROWS + 1 prefetch the
+    // next strip's rows 0 and 1 up to columns col - ROWS and col - ROWS - 1,
+    // which that strip's lanes 0 and 1 update by warp step col - ROWS - 1.
+    // (Each step's strip also reads and writes its own cells only after the
+    // previous step did, at the same warp step of the skew, which these counts
+    // cover.)
+    auto need_p0 = [&](int col) { return min(col, TW); };
+    auto need_p1 = [&](int col) { return max(0, min(col - ROWS, TW)); };
     if (!wait_deps(d, dep, min(CHUNK - 1 + ROWS, TW), need_p0(DIST + 3), need_p1(DIST + 3))) bail = true;
 
     // prime: the first three columns of this lane's row become records, then
