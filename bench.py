@@ -1021,8 +1021,9 @@ def main():
     ap.add_argument("--no-c1", action="store_true", help="skip the small CPU configuration run in full")
     ap.add_argument("--no-c1-ref", action="store_true",
                     help="in the c1 section, skip the reference program's full run")
-    ap.add_argument("--c1-in-flight", type=int, default=31,
-                    help="steps in flight of the c1 section's device-timed run")
+    ap.add_argument("--c1-in-flight", type=int, default=0,
+                    help="steps in flight of the c1 section's device-timed run (0: the library's default, "
+                         "as the program uses)")
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="arrival window of the serving sample (the configuration's: 600 s)")
     ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 120.0)
