@@ -252,6 +252,18 @@ extern "C" {
 
 const char* fx_last_error(const fx_ctx* ctx) { return ctx ? ctx->err.c_str() : g_last_error.c_str(); }
 
+// Steps in flight when the caller leaves it to the library: as many as the
+// per-step planes of h, h0, the pre-melt depth, fe_1, fn_1 and flags allow
+// within 1 GiB, at least 8 and at most 63. A launch of the ADE sweep pays the
+// wavefront's start-up (the strips and columns of the grid, once), so small
+// grids, whose sweeps are short, run far faster with many steps per launch;
+// large grids keep 8 (and the memory).
+static int default_steps_in_flight(long long plane, bool prec32) {
+  const long long per_step = plane * (5LL * (prec32 ? 4 : 8) + 1);
+  const long long k = per_step > 0 ? (1LL << 30) / per_step : FX_MAX_SLOTS - 1;
+  return (int)std::max(8LL, std::min<long long>(FX_MAX_SLOTS - 1, k));
+}
+
 int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
   if (!g || !p || !out) return fx_fail(nullptr, FX_ERR_ARG, "fx_create: null argument");
   *out = nullptr;
@@ -296,7 +308,7 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
   d.soil_rate = p->soil_release_rate;
   for (int k = 0; k < FX_MAX_CHEM; ++k) d.dcoef[k] = p->d_coef[k];
   {
-    int k = p->steps_in_flight > 0 ? p->steps_in_flight : 8;
+    int k = p->steps_in_flight > 0 ? p->steps_in_flight : default_steps_in_flight(d.plane, p->precision == 1);
     if (k > FX_MAX_SLOTS - 1) k = FX_MAX_SLOTS - 1;
     d.nslot = k + 1;  // a batch of k steps plus the state before it
     c->batch_steps = k;
@@ -425,7 +437,7 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
   // the allocations of fx_create, field by field, plus the extension grids
   const long long ld = ((g->nrows + 2 + FX_ROFF + 31) / 32) * 32;
   const long long plane = ld * (g->ncols + 2);
-  long long k = p->steps_in_flight > 0 ? p->steps_in_flight : 8;
+  long long k = p->steps_in_flight > 0 ? p->steps_in_flight : default_steps_in_flight(plane, p->precision == 1);
   if (k > FX_MAX_SLOTS - 1) k = FX_MAX_SLOTS - 1;
   const long long nslot = k + 1;
   const long long strips = (g->nrows + fx_ade_rows_per_strip() - 1) / fx_ade_rows_per_strip();

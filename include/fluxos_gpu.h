@@ -63,7 +63,8 @@ typedef struct fx_params {
   int ade;           /* EXTERNAL_MODULES.ADE_TRANSPORT.STATUS */
   int volrat_mode;   /* domain-edge weir: 0 = weir formula (default), 1 = closed */
   double d_coef[FX_MAX_CHEM]; /* dispersion coefficient per solute */
-  int steps_in_flight; /* steps whose ADE sweeps run in one launch, 1..63 (0 = 8) */
+  int steps_in_flight; /* steps whose ADE sweeps run in one launch, 1..63; 0 = as many as
+                          * the per-step planes allow within 1 GiB, from 8 to 63 */
   int precision;       /* 0 = FP64, the reference's arithmetic (default);
                           1 = FP32 state: the depth above the bed eta = z - zb and
                           the bed's differences to the east and north neighbours
