@@ -826,7 +826,7 @@ def run_serve(args, rank: int = 0, world: int = 1):
     from fluxos_cpp_b200 import serve
     reqs = serve.poisson_requests(rate=4.0, duration=args.serve_seconds, seed=4,
                                   horizon_scale=args.serve_horizon_scale)
-    srv = serve.Server(cap_bytes=150e9, chunk_steps=32)
+    srv = serve.Server(cap_bytes=150e9, chunk_steps=31)
     srv.run(serve.shard(reqs, rank, world), generate_ahead=args.serve_generate_ahead, generator_threads=8)
     part = srv.last_part
     srv.close()

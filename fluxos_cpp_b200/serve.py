@@ -59,7 +59,7 @@ class Request:
     nchem: int = 1
     extension_grids: int = 2
     precision: str = "fp32"
-    steps_in_flight: int = 8
+    steps_in_flight: int = 31  # the batch launch sweeps this many steps per ADE launch
     # filled in by the server
     inputs: Optional[S.Scenario] = None  # generated ahead of arrival
     prep_start: Optional[float] = None
@@ -87,7 +87,7 @@ class Server:
     batch and a request's domain (fx.Batch and scenarios.make_domain; tests
     of the host logic pass stand-ins)."""
 
-    def __init__(self, cap_bytes: float = 150e9, chunk_steps: int = 32, keep=(),
+    def __init__(self, cap_bytes: float = 150e9, chunk_steps: int = 31, keep=(),
                  on_output: Optional[Callable] = None, host_threads: int = 4,
                  clock: Callable[[], float] = time.perf_counter,
                  batch_factory: Optional[Callable] = None, make_domain: Optional[Callable] = None):
