@@ -1026,7 +1026,7 @@ def main():
                          "as the program uses)")
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="arrival window of the serving sample (the configuration's: 600 s)")
-    ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 120.0)
+    ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 80.0)
     ap.add_argument("--serve-generate-ahead", type=float, default=3.0,
                     help="seconds before arrival at which a request's inputs are generated")
     args = ap.parse_args()
