@@ -814,6 +814,43 @@ def run_dambreak(args) -> dict:
     return out
 
 
+def serve_accuracy(reqs: list, count: int) -> dict:
+    """The FP32 error of served requests: the `count` smallest run alone to
+    their horizons (the same states as in the batch: the serving test checks
+    that each result is bit-identical alone and in the mix) in FP32, FP64 and
+    two FP64 copies with depths perturbed by a relative 1e-7; the relative L1
+    depth error of FP32 and of the perturbed runs against FP64."""
+    from fluxos_cpp_b200 import accuracy as A
+    from fluxos_cpp_b200 import scenarios as S
+    rows = []
+    for r in sorted(reqs, key=lambda x: x.cells)[:count]:
+        sc = r.make()
+        runs = [S.make_domain(sc, precision="fp32", steps_in_flight=r.steps_in_flight),
+                S.make_domain(sc, precision="fp64", steps_in_flight=r.steps_in_flight)]
+        runs += [_perturbed(sc, seed, in_flight=r.steps_in_flight) for seed in (0, 1)]
+        w0 = [d.mass()[0] for d in runs]
+        for d in runs:
+            while True:
+                st = d.step(512)
+                if st["print_pending"]:
+                    d.print_done()
+                if st["finished"]:
+                    break
+        e32 = A.state_errors(runs[0], runs[1], sc.ks)
+        ep = [A.state_errors(d, runs[1], sc.ks)["depth"]["l1_rel"] for d in runs[2:]]
+        rows.append({"request": r.rid, "cells": r.cells, "horizon_s": sc.horizon, "solutes": sc.nchem,
+                     "steps": int(runs[0].status()["steps"]),
+                     "fp32_depth_l1_rel": e32["depth"]["l1_rel"], "fp32_depth_linf_m": e32["depth"]["linf_abs"],
+                     "fp32_discharge_l1_rel": e32["discharge"]["l1_rel"],
+                     "perturbed_fp64_depth_l1_rel": ep,
+                     "fp32_mass_rel_err": A.water_balance(runs[0], w0[0])["rel_err"],
+                     "fp64_mass_rel_err": A.water_balance(runs[1], w0[1])["rel_err"]})
+        for d in runs:
+            d.close()
+    return {"what": "the smallest requests run alone to their horizons: FP32, and two FP64 runs with depths "
+                    "perturbed by a relative 1e-7, against FP64", "requests": rows}
+
+
 def run_serve(args, rank: int = 0, world: int = 1):
     """The serving configuration's request stream (Poisson arrivals at
     4/s, seed 4, grids 128^2-4096^2, 1-12 h horizons, 1-3 solutes, FP32,
@@ -838,6 +875,7 @@ def run_serve(args, rank: int = 0, world: int = 1):
     if rank != 0:
         return None
     stats = serve.summarize(parts)
+    stats["accuracy_sample"] = serve_accuracy(reqs, args.serve_accuracy_requests)
     # the load the configuration's full horizons would offer: the same
     # requests' measured steps per simulated second, over unscaled horizons
     full_offer = (stats["offered_cell_updates_per_s"] / args.serve_horizon_scale
@@ -1027,6 +1065,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="arrival window of the serving sample (the configuration's: 600 s)")
     ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 80.0)
+    ap.add_argument("--serve-accuracy-requests", type=int, default=3,
+                    help="served requests also run alone in FP64 and perturbed FP64 for their error")
     ap.add_argument("--serve-generate-ahead", type=float, default=3.0,
                     help="seconds before arrival at which a request's inputs are generated")
     args = ap.parse_args()
