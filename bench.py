@@ -1064,7 +1064,7 @@ def main():
                          "as the program uses)")
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="arrival window of the serving sample (the configuration's: 600 s)")
-    ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 80.0)
+    ap.add_argument("--serve-horizon-scale", type=float, default=1.0 / 100.0)
     ap.add_argument("--serve-accuracy-requests", type=int, default=3,
                     help="served requests also run alone in FP64 and perturbed FP64 for their error")
     ap.add_argument("--serve-generate-ahead", type=float, default=3.0,

@@ -607,9 +607,39 @@ int fx_download(fx_ctx* c, const char* field, double* host) {
   return get_grid(c, src, f.f32, host);
 }
 
+// The flag byte of each grid cell from the two uploaded float planes (1.0 =
+// set), into plane 0 of the flags; padding rows are left as they are.
+__global__ void k_flags_of(const float* __restrict__ ldry, const float* __restrict__ wall, uint8_t* __restrict__ fl,
+                           int ld, int mr, long long plane) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i % ld) - FX_ROFF;
+    if (r < 0 || r >= mr) continue;
+    fl[i] = (uint8_t)((ldry[i] == 1.0f ? FX_F_LDRY : 0) | (wall[i] == 1.0f ? FX_F_WALL : 0));
+  }
+}
+
 int fx_upload_flags(fx_ctx* c, const float* ldry, const float* wall) {
   if (!c || !ldry || !wall) return fx_fail(c, FX_ERR_ARG, "fx_upload_flags: null argument");
   const int mr = c->d.nr + 2, mc = c->d.nc + 2;
+  if (c->d.nslot >= 9) {
+    // The two float planes cross the bus as they are, into the last 8 slot
+    // planes of the flags (4 bytes per cell each), are combined on the device
+    // into plane 0, which is then copied over the others.
+    const size_t pl = (size_t)c->d.plane;
+    float* sl = reinterpret_cast<float*>(c->d.flags + pl * (c->d.nslot - 8));
+    float* sw = reinterpret_cast<float*>(c->d.flags + pl * (c->d.nslot - 4));
+    for (int q = 0; q < 2; ++q)
+      FX_CK(c, cudaMemcpy2DAsync((q ? sw : sl) + FX_ROFF, (size_t)c->d.ld * sizeof(float), q ? wall : ldry,
+                                 (size_t)mr * sizeof(float), (size_t)mr * sizeof(float), (size_t)mc,
+                                 cudaMemcpyHostToDevice, c->stream));
+    k_flags_of<<<plane_grid(c->d.plane), 256, 0, c->stream>>>(sl, sw, c->d.flags, c->d.ld, mr, c->d.plane);
+    FX_CK(c, cudaGetLastError());
+    for (int k = 1; k < c->d.nslot; ++k)
+      FX_CK(c, cudaMemcpyAsync(c->d.flags + k * pl, c->d.flags, pl, cudaMemcpyDeviceToDevice, c->stream));
+    FX_CK(c, cudaStreamSynchronize(c->stream));
+    c->prepared = false;
+    return FX_OK;
+  }
   std::vector<uint8_t> fl((size_t)mr * mc);
   for (size_t i = 0; i < fl.size(); ++i)
     fl[i] = (uint8_t)((ldry[i] == 1.0f ? FX_F_LDRY : 0) | (wall[i] == 1.0f ? FX_F_WALL : 0));
