@@ -808,7 +808,7 @@ int fx_prepare(fx_ctx* c) {
       c->z_pending = false;
     }
   }
-  fx_launch_mark_static(c->d_dev, 0, c->stream);
+  fx_launch_mark_static(c->d_dev, 0, c->d.plane, c->stream);
   fx_launch_courant_scan(c->d_dev, c->d_tiles, c->ntiles, c->d.tile_rows, c->stream);
   FX_CK(c, cudaGetLastError());
   FX_CK(c, cudaStreamSynchronize(c->stream));

@@ -1951,18 +1951,29 @@ __global__ void k_batch_begin(const fx_dev* __restrict__ devs, int ndom) {
 }
 
 // Sets the bed flags that never change (NODATA bed) in every slot plane.
+// One thread per 4 cells of a column (ld is a multiple of 32, so the 4 share
+// the column): the four flags bytes of a slot move as one 32-bit word.
 __global__ void k_mark_static(const fx_dev* __restrict__ devs, int dom) {
   const fx_dev& d = devs[dom];
-  const long long n = d.plane;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int icol = (int)(i / d.ld), irow = (int)(i % d.ld) - FX_ROFF;
-    if (irow < 1 || irow > d.nr || icol < 1 || icol > d.nc) continue;
-    const bool nod = d.zb[i] == d.nodata;
-    for (int k = 0; k < d.nslot; ++k) {
-      uint8_t& f = d.flags[k * d.plane + i];
-      f = (uint8_t)((f & ~FX_F_NODATA) | (nod ? FX_F_NODATA : 0));
-    }
+  const long long i = 4 * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
+  if (i >= d.plane) return;
+  const int icol = (int)(i / d.ld), irow0 = (int)(i - (long long)icol * d.ld) - FX_ROFF;
+  if (icol < 1 || icol > d.nc) return;
+  const double2 z01 = *reinterpret_cast<const double2*>(d.zb + i);
+  const double2 z23 = *reinterpret_cast<const double2*>(d.zb + i + 2);
+  const double zb[4] = {z01.x, z01.y, z23.x, z23.y};
+  unsigned keep = 0xffffffffu, set = 0u;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int irow = irow0 + j;
+    if (irow < 1 || irow > d.nr) continue;
+    keep &= ~((unsigned)FX_F_NODATA << (8 * j));
+    if (zb[j] == d.nodata) set |= (unsigned)FX_F_NODATA << (8 * j);
   }
+  if (keep == 0xffffffffu) return;
+  unsigned* f = reinterpret_cast<unsigned*>(d.flags + i);
+  const long long step = d.plane / 4;
+  for (int k = 0; k < d.nslot; ++k) f[k * step] = (f[k * step] & keep) | set;
 }
 
 // FP32 state: the compensated depth (eta, eta_lo) = z - zb over the whole
@@ -2022,8 +2033,8 @@ void fx_launch_finalize(const fx_dev* devs, int ndom, cudaStream_t s) {
 void fx_launch_batch_begin(const fx_dev* devs, int ndom, cudaStream_t s) {
   fx::k_batch_begin<<<(ndom + 127) / 128, 128, 0, s>>>(devs, ndom);
 }
-void fx_launch_mark_static(const fx_dev* devs, int dom, cudaStream_t s) {
-  fx::k_mark_static<<<592, 256, 0, s>>>(devs, dom);
+void fx_launch_mark_static(const fx_dev* devs, int dom, long long plane, cudaStream_t s) {
+  fx::k_mark_static<<<(unsigned)((plane / 4 + 255) / 256), 256, 0, s>>>(devs, dom);
 }
 namespace {
 template <int BY>

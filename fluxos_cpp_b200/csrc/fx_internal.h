@@ -64,7 +64,8 @@ void fx_fill_status(const fx_ctl& k, fx_status* st);
 // domain descriptors; the *_one forms take one domain's descriptor by value.
 void fx_launch_finalize(const fx_dev* devs, int ndom, cudaStream_t s);
 void fx_launch_batch_begin(const fx_dev* devs, int ndom, cudaStream_t s);
-void fx_launch_mark_static(const fx_dev* devs, int dom, cudaStream_t s);
+// plane: the domain's elements per field (fx_dev::plane)
+void fx_launch_mark_static(const fx_dev* devs, int dom, long long plane, cudaStream_t s);
 void fx_launch_hydro(const fx_dev* devs, const fx_tile* tiles, int ntiles, bool prec32, int tile_rows,
                      cudaStream_t s);
 void fx_launch_hydro_one(const fx_dev& d, cudaStream_t s);
