@@ -316,35 +316,53 @@ int fx_batch_autotune(fx_batch* b, int trial_steps, int* tile_rows, int* steps_i
   int kmax = FX_MAX_SLOTS - 1;
   for (fx_ctx* c : b->doms) kmax = std::min(kmax, c->batch_steps);
   // warm-up of the current configuration (first graph, caches)
-  double rate = 0, best = -1;
+  double rate = 0;
   int rc = trial(b, trial_steps, &rate);
   if (rc) return rc;
-  int best_rows = b->tile_rows;
-  for (int r : {4, 8, 16}) {
-    b->tile_rows = r;
-    b->dirty = true;
-    if ((rc = trial(b, 1, &rate))) return rc;  // rebuilds the tables and the graph
-    if ((rc = trial(b, trial_steps, &rate))) return rc;
-    if (rate > best) {
-      best = rate;
-      best_rows = r;
+  // Each choice is tried twice, in one order and then in the reverse order,
+  // and scored by the sum of its two times per cell-step: the members' state
+  // changes as the trials advance it, and a drift linear in the step count
+  // adds the same to every score.
+  auto sweep = [&](const int* vals, int nv, auto apply, auto steps_for, int* best_val) -> int {
+    double score[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool ok[8] = {false, false, false, false, false, false, false, false};
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int q = 0; q < nv; ++q) {
+        const int j = pass == 0 ? q : nv - 1 - q;
+        apply(vals[j]);
+        int rc2 = trial(b, 1, &rate);  // rebuilds the tables and the graph
+        if (rc2) return rc2;
+        if ((rc2 = trial(b, steps_for(vals[j]), &rate))) return rc2;
+        if (rate > 0) {
+          score[j] += 1.0 / rate;
+          ok[j] = pass == 0 ? true : ok[j];
+        } else {
+          ok[j] = false;
+        }
+      }
     }
-  }
+    double lo = -1;
+    for (int j = 0; j < nv; ++j)
+      if (ok[j] && (lo < 0 || score[j] < lo)) {
+        lo = score[j];
+        *best_val = vals[j];
+      }
+    return FX_OK;
+  };
+  int best_rows = b->tile_rows;
+  const int rows[3] = {4, 8, 16};
+  rc = sweep(rows, 3, [&](int r) { b->tile_rows = r; b->dirty = true; }, [&](int) { return trial_steps; },
+             &best_rows);
+  if (rc) return rc;
   b->tile_rows = best_rows;
   b->dirty = true;
   int best_k = std::min(b->k_limit, kmax);
-  best = -1;
-  for (int k : {2, 4, 8, 16, 31, 63}) {
-    if (k > kmax) continue;
-    b->k_limit = k;
-    b->dirty = true;
-    if ((rc = trial(b, 1, &rate))) return rc;
-    if ((rc = trial(b, std::max(trial_steps, 2 * k), &rate))) return rc;
-    if (rate > best) {
-      best = rate;
-      best_k = k;
-    }
-  }
+  int ks[6], nk = 0;
+  for (int k : {2, 4, 8, 16, 31, 63})
+    if (k <= kmax) ks[nk++] = k;
+  rc = sweep(ks, nk, [&](int k) { b->k_limit = k; b->dirty = true; },
+             [&](int k) { return std::max(trial_steps, 2 * k); }, &best_k);
+  if (rc) return rc;
   b->k_limit = best_k;
   b->dirty = true;
   if (tile_rows) *tile_rows = best_rows;

@@ -1032,25 +1032,40 @@ int fx_time_steps(fx_ctx* c, int n, double* ms_total, double* ms_hydro, double* 
 int fx_autotune(fx_ctx* c, int trial_steps, int* tile_rows) {
   if (!c || trial_steps < 1) return fx_fail(c, FX_ERR_ARG, "fx_autotune: bad argument");
   // Each candidate runs trial_steps real steps (results do not depend on the
-  // tile shape); the hydrodynamic kernel time per step decides.
+  // tile shape); the hydrodynamic kernel time per step decides. The state
+  // changes as the run advances (a spreading wet front makes later steps
+  // dearer), so the candidates run twice, in one order and then in the
+  // reverse order, and each is scored by the sum of its two times per step:
+  // a drift that is linear in the step count adds the same to every score.
   const int cand[3] = {4, 8, 16};
+  double ms[3] = {0.0, 0.0, 0.0};
+  bool ok[3] = {true, true, true};
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int q = 0; q < 3; ++q) {
+      const int j = pass == 0 ? q : 2 - q;
+      int rc = set_tile_rows(c, cand[j]);
+      if (rc) return rc;
+      rc = read_ctl(c);
+      if (rc) return rc;
+      const long long s0 = c->ctl_host->steps;
+      double tot = 0, hyd = 0, ade = 0;
+      rc = fx_time_steps(c, trial_steps, &tot, &hyd, &ade);
+      if (rc) return rc;
+      const long long ran = c->ctl_host->steps - s0;
+      if (ran < 1) {  // the run stopped (output due or over): nothing measured
+        ok[j] = false;
+        continue;
+      }
+      ms[j] += hyd / (double)ran;
+    }
+  }
   double best_ms = 0.0;
   int best = c->d.tile_rows;
-  for (int r : cand) {
-    int rc = set_tile_rows(c, r);
-    if (rc) return rc;
-    rc = read_ctl(c);
-    if (rc) return rc;
-    const long long s0 = c->ctl_host->steps;
-    double tot = 0, hyd = 0, ade = 0;
-    rc = fx_time_steps(c, trial_steps, &tot, &hyd, &ade);
-    if (rc) return rc;
-    const long long ran = c->ctl_host->steps - s0;
-    if (ran < 1) continue;  // the run stopped (output due or over): nothing measured
-    const double ms = hyd / (double)ran;
-    if (best_ms == 0.0 || ms < best_ms) {
-      best_ms = ms;
-      best = r;
+  for (int j = 0; j < 3; ++j) {
+    if (!ok[j]) continue;
+    if (best_ms == 0.0 || ms[j] < best_ms) {
+      best_ms = ms[j];
+      best = cand[j];
     }
   }
   int rc = set_tile_rows(c, best);

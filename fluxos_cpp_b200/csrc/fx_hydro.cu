@@ -673,16 +673,31 @@ __device__ __forceinline__ float div_dxy_f(const fx_dev& d, float x) {
   return d.dxy_pow2 ? x * (float)d.inv_dxy : fdiv(x, (float)d.dxy);
 }
 
+// The Roe face-depth test of the FP32 state, `.5 * (max(0, dP) + max(0, dQ))
+// > hdry` on the two cells' compensated FP64 depths, decided from its FP32
+// value x = .5f * (max(0, eta_P) + max(0, eta_Q)) where that is safe: each
+// eta differs from its compensated depth by at most half an ulp and the sum
+// rounds once, so |x - exact| <= x * 2^-23, and outside the band
+// [hdry (1 - 2^-19), hdry (1 + 2^-19)] (bounds rounded to float) x and the
+// exact value lie on the same side of hdry. Inside the band the FP64 test
+// (`exact`) decides. The outcome is the FP64 test's in every case.
+template <class F>
+__device__ __forceinline__ bool above_hdry(float x, float lo, float hi, F exact) {
+  if (x > hi) return true;
+  if (x < lo) return false;
+  return exact();
+}
+
 template <class SM>
 __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int irow, int icol,
                              float dtl, float out[6]) {
   const double hdry = d.hdry;
   const float hdryl = (float)d.hdry, gaccl = (float)d.gaccl;
+  const float hdry_lo = (float)(hdry * (1.0 - 0x1p-19)), hdry_hi = (float)(hdry * (1.0 + 0x1p-19));
   const int P = sidx(sr, sc), W = sidx(sr - 1, sc), E = sidx(sr + 1, sc);
   const int Sx = sidx(sr, sc - 1), N = sidx(sr, sc + 1);
   const int ES = sidx(sr + 1, sc - 1), EN = sidx(sr + 1, sc + 1), WN = sidx(sr - 1, sc + 1);
   auto ksat = [&](int k) { return (S.cls[k] & C_INT) ? (float)d.ks : 0.0f; };
-  auto hat = [&](int k) { return fmaxf(0.0f, S.eta[k]); };
   const float kspl = ksat(P);
   const float nueml = (float)d.nueml;
   const float dx = (float)d.dxy, dy = dx;
@@ -692,9 +707,9 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   // bed differences: exact in FP64 for the branch tests, rounded for the flux arithmetic
   const double sx_d = S.zb[E] - S.zb[P], sy_d = S.zb[N] - S.zb[P];
   const float etap = S.eta[P], sxp = (float)sx_d, syp = (float)sy_d;
-  // compensated depths for the branch tests (FP64, as the FP64 path decides them)
-  const double dP = fx_dd_val(etap, S.eta_lo[P]), dE = fx_dd_val(S.eta[E], S.eta_lo[E]);
-  const double dN = fx_dd_val(S.eta[N], S.eta_lo[N]);
+  // compensated depths for the branch tests (FP64, as the FP64 path decides
+  // them), formed where a test needs them
+  auto dd = [&](int k) { return fx_dd_val(S.eta[k], S.eta_lo[k]); };
   float qp = S.qx[P], qe = S.qx[E], qn = S.qx[N];
   float rw = S.qy[W], rp = S.qy[P], re = S.qy[E], rn = S.qy[N];
   const float hp = fmaxf(0.0f, etap);
@@ -712,6 +727,7 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   if (lde_dry) {
     hme = fmaxf(0.0f, etap - .5f * sxp);
     he = qe = re = 0.0f;
+    const double dP = dd(P), dE = dd(E);
     const double dze_d = sx_d + (dE - dP);
     if (fmax(0.0, dP - .5 * sx_d) > hdry) {
       if (dze_d >= 0.0) {
@@ -731,6 +747,7 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   if (ldn_dry) {
     hmn = fmaxf(0.0f, etap - .5f * syp);
     hn = qn = rn = 0.0f;
+    const double dP = dd(P), dN = dd(N);
     const double dzn_d = sy_d + (dN - dP);
     if (fmax(0.0, dP - .5 * sy_d) > hdry) {
       if (dzn_d >= 0.0) {
@@ -773,7 +790,7 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   float fe1r = 0.f, fe2r = 0.f, fe3r = 0.f, fn1r = 0.f, fn2r = 0.f, fn3r = 0.f;
   if (lroe) {
     float cc;
-    if (.5 * (fmax(0.0, dP) + fmax(0.0, dE)) > hdry) {
+    if (above_hdry(hme, hdry_lo, hdry_hi, [&] { return .5 * (fmax(0.0, dd(P)) + fmax(0.0, dd(E))) > hdry; })) {
       float dzea = fabsf(dze);
       if (dzea > 0.5f * hme) {
         dzea = fminf(dzea, fabsf(he - hp));
@@ -788,7 +805,8 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
     fe1r = -((c2 * c3a - c2a * c3) * dze + (c2a - c3a) * dqe) * cc;
     fe2r = -(c2 * c3 * (c3a - c2a) * dze + (c2a * c2 - c3a * c3) * dqe) * cc;
     fe3r = -(vme * (c2 * c3a - 2.f * cme * c1a - c2a * c3) * dze + vme * (c2a - c3a) * dqe + 2.f * cme * c1a * dre) * cc;
-    if (!ldp_dry && .5 * (fmax(0.0, dP) + fmax(0.0, dN)) > hdry) {
+    if (!ldp_dry &&
+        above_hdry(hmn, hdry_lo, hdry_hi, [&] { return .5 * (fmax(0.0, dd(P)) + fmax(0.0, dd(N))) > hdry; })) {
       float dzna = fminf(fabsf(dzn), fabsf(hn - hp));
       dzn = copysignf(dzna, dzn);
       cc = fdiv(.25f, cmn);
@@ -811,9 +829,11 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
   float fn1 = fn1c + fn1r;
   const float fn2 = fn2c + fn2r;
   const float fn3 = fn3c + fn3r + .5f * gaccl * (hmn * hmn);
-  const float weir = fsqrt(gaccl) * hp * fsqrt(hp);
-  if (icol == 1 || icol == d.nc) fn1 = fminf(volrat, weir);
-  if (irow == 1 || irow == d.nr) fe1 = fminf(volrat, weir);
+  if (icol == 1 || icol == d.nc || irow == 1 || irow == d.nr) {  // the edge weir, on edge cells only
+    const float weir = fsqrt(gaccl) * hp * fsqrt(hp);
+    if (icol == 1 || icol == d.nc) fn1 = fminf(volrat, weir);
+    if (irow == 1 || irow == d.nr) fe1 = fminf(volrat, weir);
+  }
   volrat = fdiv((float)d.arbase * hp, dtl);
   if (volrat > 0.0f) {
     if (fe1 > 0.0f && fn1 > 0.0f) {

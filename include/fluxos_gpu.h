@@ -173,8 +173,10 @@ int fx_time_steps(fx_ctx* ctx, int nsteps, double* ms_total, double* ms_hydro, d
  * fx_status, water(t) - water(0) = budget_melt - budget_out up to rounding. */
 int fx_mass(fx_ctx* ctx, double* water, double* solute_mass);
 /* Autotuner: runs trial_steps real steps with each tile shape (tile_rows 4,
- * 8, 16), keeps the one whose hydrodynamic kernel took least time per step
- * and returns it in *tile_rows (may be NULL). */
+ * 8, 16), twice (in that order, then in the reverse order, so a state that
+ * grows dearer as the trials advance it favours no shape), keeps the one
+ * whose hydrodynamic kernel took least time per step over both runs and
+ * returns it in *tile_rows (may be NULL). */
 int fx_autotune(fx_ctx* ctx, int trial_steps, int* tile_rows);
 
 /* --- batches --------------------------------------------------------------
@@ -206,8 +208,9 @@ void* fx_batch_stream(fx_batch* b);
 int fx_batch_set_option(fx_batch* b, const char* name, long long value);
 /* Autotuner of the batch: tries each tile shape, then each steps-in-flight
  * bound (2, 4, 8, 16, 31, 63, up to the members' own), for trial_steps real
- * steps of all members, keeps the fastest
- * (cell-steps per second) and returns the choice (pointers may be NULL). */
+ * steps of all members (at least 2 x the bound), each twice (in that order,
+ * then in the reverse order), keeps the fastest over both runs (time per
+ * cell-step) and returns the choice (pointers may be NULL). */
 int fx_batch_autotune(fx_batch* b, int trial_steps, int* tile_rows, int* steps_in_flight);
 
 /* --- allocation-free ADE sweep -------------------------------------------

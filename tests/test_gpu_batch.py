@@ -112,7 +112,8 @@ def test_tile_shapes_staging_and_autotuner_keep_results(precision):
             assert np.array_equal(d.download(k), v), (r, tma, k)
         d.close()
     d = S.make_domain(sc, precision=precision, steps_in_flight=4)
-    assert d.autotune(8) in (4, 8, 16)
+    assert d.autotune(4) in (4, 8, 16)  # 3 shapes x 2 runs x 4 real steps
+    assert d.status()["steps"] == 24
     d.step(40 - d.status()["steps"])
     assert d.status()["steps"] == 40
     for k, v in want.items():
