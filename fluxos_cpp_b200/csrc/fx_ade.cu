@@ -75,6 +75,16 @@ struct Ring {
   unsigned fl[RING][32]; // the 4-byte word holding the cell's flag byte
 };
 
+// The FP32 state's ring: the concentration group and the cell's per-step
+// record (fx_dev::rec32), two 16-byte copies from one 32-byte sector.
+template <>
+struct Ring<float> {
+  static constexpr int CV = 4;
+  float c[RING][32][CV];
+  float4 a[RING][32];  // h0, h, hp, melt multiplier
+  float4 b[RING][32];  // fe_1, fn_1, flag byte (as the float's bits), 0
+};
+
 template <class T>
 struct Rec {
   T c;   // concentration before the sweep (after dilution, before re-scale)
@@ -101,11 +111,6 @@ struct Fields<double> {
 };
 template <>
 struct Fields<float> {
-  static __device__ __forceinline__ const float* h(const fx_dev& d) { return d.h_f; }
-  static __device__ __forceinline__ const float* h0(const fx_dev& d) { return d.h0_f; }
-  static __device__ __forceinline__ const float* hpm(const fx_dev& d) { return d.hpm_f; }
-  static __device__ __forceinline__ const float* fe1(const fx_dev& d) { return d.fe1_f; }
-  static __device__ __forceinline__ const float* fn1(const fx_dev& d) { return d.fn1_f; }
   static __device__ __forceinline__ const float* mm(const fx_dev& d) { return d.melt_mult_f; }
   static __device__ __forceinline__ float* conc(const fx_dev& d) { return d.conc_f; }
   static __device__ __forceinline__ float* soil(const fx_dev& d) { return d.soil_f; }
@@ -151,34 +156,21 @@ struct StepIn {
   bool wintra;          // the soil release follows the sweep (hpall != 0)
 };
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
-  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = valid ? 8 : 0;  // 0 source bytes: the slot is zero-filled
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
-}
-template <int B>
-__device__ __forceinline__ void cp_async_n(void* smem, const void* gmem, bool valid) {
-  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = valid ? B : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(gmem), "n"(B), "r"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {
-  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = valid ? 4 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem, bool valid) {
-  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = valid ? 16 : 0;
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
-}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Issue the copies of cell (ix, iy) into ring slot `slot` of this lane.
+// Issue the copies of cell (ix, iy) into ring slot `slot` of this lane. The
+// shared and global addresses are formed once per cell (a 32-bit shared
+// address of the lane's entry, one offset into the slot plane); a cell
+// outside the grid copies 0 source bytes, which zero-fills its entries.
+__device__ __forceinline__ void cp_async_sz(unsigned dst, const void* gmem, int n, int bytes) {
+  if (bytes == 16) asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(gmem), "r"(n));
+  else if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(gmem), "r"(n));
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(gmem), "r"(n));
+}
 template <class T>
 __device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const T* A, Ring<T>& R, int lane,
                                          int ix, int iy) {
@@ -187,16 +179,33 @@ __device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const
   const int slot = iy & (RING - 1);
   const bool inr = ix >= 0 && ix <= d.nr + 1 && iy >= 0 && iy <= d.nc + 1;
   const long long gi = inr ? fx_ix(d, ix, iy) : 0;
-  cp_async16_cg(&R.c[slot][lane][0], A + (gi & ~(long long)(Ring<T>::CV - 1)), inr);
-  cp_async_n<B>(&R.h0[slot][lane], F::h0(d) + S.cur + gi, inr);
-  cp_async_n<B>(&R.h[slot][lane], F::h(d) + S.cur + gi, inr);
-  cp_async_n<B>(&R.hp[slot][lane], S.dilute ? (const void*)(F::hpm(d) + S.cur + gi) : (const void*)F::h(d),
-                inr && S.dilute);
-  const bool mm_ok = inr && S.dilute && F::mm(d) != nullptr;
-  cp_async_n<B>(&R.mm[slot][lane], mm_ok ? (const void*)(F::mm(d) + gi) : (const void*)F::h(d), mm_ok);
-  cp_async_n<B>(&R.fe1[slot][lane], F::fe1(d) + S.cur + gi, inr);
-  cp_async_n<B>(&R.fn1[slot][lane], F::fn1(d) + S.cur + gi, inr);
-  cp_async4(&R.fl[slot][lane], d.flags + S.cur + (gi & ~3LL), inr);
+  const long long o = S.cur + gi;
+  // the concentration is written during the launch by other warps: through L2 only
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(&R.c[slot][lane][0])),
+               "l"(A + (gi & ~(long long)(Ring<T>::CV - 1))), "r"(inr ? 16 : 0));
+  if constexpr (B == 4) {
+    const float4* rec = d.rec32 + 2 * o;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(&R.a[slot][lane])),
+                 "l"(rec), "r"(inr ? 16 : 0));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(&R.b[slot][lane])),
+                 "l"(rec + 1), "r"(inr ? 16 : 0));
+  } else {
+    const int nb = inr ? B : 0;
+    const unsigned e = (unsigned)__cvta_generic_to_shared(&R) + (unsigned)(slot * 32 + lane) * B;
+    cp_async_sz(e + (unsigned)offsetof(Ring<T>, h0), F::h0(d) + o, nb, B);
+    cp_async_sz(e + (unsigned)offsetof(Ring<T>, h), F::h(d) + o, nb, B);
+    const bool dil = S.dilute;
+    cp_async_sz(e + (unsigned)offsetof(Ring<T>, hp), dil ? F::hpm(d) + o : F::h(d), dil ? nb : 0, B);
+    const bool mm_ok = dil && F::mm(d) != nullptr;
+    cp_async_sz(e + (unsigned)offsetof(Ring<T>, mm), mm_ok ? F::mm(d) + gi : F::h(d), mm_ok ? nb : 0, B);
+    cp_async_sz(e + (unsigned)offsetof(Ring<T>, fe1), F::fe1(d) + o, nb, B);
+    cp_async_sz(e + (unsigned)offsetof(Ring<T>, fn1), F::fn1(d) + o, nb, B);
+    // the 4-byte word holding the flag byte (slot planes are multiples of 32 bytes)
+    cp_async_sz((unsigned)__cvta_generic_to_shared(&R.fl[slot][lane]), d.flags + (o & ~3LL), inr ? 4 : 0, 4);
+  }
 }
 
 // The same record with the tests as branches (the FP64 state: lanes skip the
@@ -258,33 +267,31 @@ __device__ __forceinline__ Rec<T> make_rec_br(const fx_dev& d, const StepIn& S, 
 // ring entry, so it is read for every (ix, iy) and the values are selected:
 // per-cell tests become selects and the block has no divergent branch (the
 // step's dilution and point inflow are the same for the whole warp). Used by
-// the FP32 state, whose divisions are a few fused operations.
+// the FP32 state, whose divisions are a few fused operations; its ring holds
+// the cell's per-step record (fx_dev::rec32).
 template <class T>
 __device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, const Ring<T>& R, int lane, int ix,
                                            int iy) {
+  static_assert(sizeof(T) == 4, "the select form reads the FP32 ring");
   const bool inr = ix >= 0 && ix <= d.nr + 1 && iy >= 0 && iy <= d.nc + 1;
   const bool interior = ix >= 1 && ix <= d.nr && iy >= 1 && iy <= d.nc;
   const int slot = iy & (RING - 1);
   const long long gi = fx_ix(d, ix, iy);  // an index into the ring's groups only, outside the grid
-  const unsigned fl = (R.fl[slot][lane] >> (8 * (unsigned)(gi & 3))) & 0xffu;
+  const float4 ra = R.a[slot][lane], rb = R.b[slot][lane];
+  const unsigned fl = __float_as_uint(rb.z);
   const int ld = fl & FX_F_LDRY;
   const bool ldp = (fl & FX_F_LDRY_PREV) != 0;
-  const T h = R.h[slot][lane];
-  const T h0 = R.h0[slot][lane];
+  const T h = ra.y;
+  const T h0 = ra.x;
   T c = R.c[slot][lane][gi & (Ring<T>::CV - 1)];
   // the inflow cell holds h0 only after its inflow; the melt's dilution
   // divides by the depth after the melt (common.cpp:226-234, 313-325)
   const bool inflow_cell = S.inflow_gi >= 0 && interior && gi == S.inflow_gi;
   const T hm = inflow_cell ? (T)S.inflow_hm : h0;
   if (S.dilute) {
-    const T hp = R.hp[slot][lane];
-    // the melt depth the hydrodynamic step added (FP32 state: melt32 in fx_hydro.cu)
-    T mi;
-    if constexpr (sizeof(T) == 4)
-      mi = Fields<T>::mm(d) ? (T)(S.meteoi * (double)R.mm[slot][lane]) : (T)S.meteoi;
-    else
-      mi = Fields<T>::mm(d) ? (T)((double)S.meteo_rate * (double)R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
-                            : (T)S.meteoi;
+    const T hp = ra.z;
+    // the melt depth the hydrodynamic step added (melt32 in fx_hydro.cu)
+    const T mi = Fields<T>::mm(d) ? (T)(S.meteoi * (double)ra.w) : (T)S.meteoi;
     const bool use = !(fl & FX_F_NODATA) && hp != T(0);  // then hm >= hp > 0
     const T cd = tdiv(c * hp + (mi * (T)S.mconc), use ? hm : T(1));
     c = use ? cd : c;
@@ -304,8 +311,8 @@ __device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, con
   r.h = inr ? h : T(0);
   r.c = interior ? c : T(0);
   r.b = interior ? b : T(0);
-  r.qx = interior ? R.fe1[slot][lane] : T(0);
-  r.qy = interior ? R.fn1[slot][lane] : T(0);
+  r.qx = interior ? rb.x : T(0);
+  r.qy = interior ? rb.y : T(0);
   r.ld = interior ? ld : 0;
   return r;
 }

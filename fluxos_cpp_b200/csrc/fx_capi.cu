@@ -48,6 +48,7 @@ struct FieldRef {
   bool slot = false;  // one plane per slot
   bool pair = false;  // two planes, the current one is fx_pp(steps)
   int copies = 1;     // identical planes (the soil mass: one per solute)
+  int rec = -1;       // FP32 per-step field: its component of the slot records (FX_R_*)
 };
 
 static FieldRef field_ref(fx_ctx* c, const char* name) {
@@ -60,18 +61,23 @@ static FieldRef field_ref(fx_ctx* c, const char* name) {
     r.slot = slot;
     r.pair = pair;
   };
+  // a per-step field: FP64 slot planes, or a component of the FP32 slot records
+  auto pick_rec = [&](void* p64, int comp) {
+    pick(p64, d.rec32, true);
+    if (p32) r.rec = comp;
+  };
   if (!strcmp(name, "zb")) r.ptr = d.zb;  // FP64 in both forms
   else if (!strcmp(name, "z")) {
     if (!p32) pick(d.z, nullptr, false, true);  // FP32: held as eta, see fx_upload / fx_download
-  } else if (!strcmp(name, "h")) pick(d.h, d.h_f, true);
+  } else if (!strcmp(name, "h")) pick_rec(d.h, FX_R_H);
   else if (!strcmp(name, "qx")) pick(d.qx, d.qx_f, false, true);
   else if (!strcmp(name, "qy")) pick(d.qy, d.qy_f, false, true);
   else if (!strcmp(name, "twet")) pick(d.twet, d.twet_f, false);
-  else if (!strcmp(name, "h0")) pick(d.h0, d.h0_f, true);
-  else if (!strcmp(name, "fe_1")) pick(d.fe1, d.fe1_f, true);
+  else if (!strcmp(name, "h0")) pick_rec(d.h0, FX_R_H0);
+  else if (!strcmp(name, "fe_1")) pick_rec(d.fe1, FX_R_FE1);
   else if (!strcmp(name, "fe_2")) pick(d.fe2, d.fe2_f, false);
   else if (!strcmp(name, "fe_3")) pick(d.fe3, d.fe3_f, false);
-  else if (!strcmp(name, "fn_1")) pick(d.fn1, d.fn1_f, true);
+  else if (!strcmp(name, "fn_1")) pick_rec(d.fn1, FX_R_FN1);
   else if (!strcmp(name, "fn_2")) pick(d.fn2, d.fn2_f, false);
   else if (!strcmp(name, "fn_3")) pick(d.fn3, d.fn3_f, false);
   else if (!strncmp(name, "conc", 4)) {
@@ -259,7 +265,8 @@ const char* fx_last_error(const fx_ctx* ctx) { return ctx ? ctx->err.c_str() : g
 // grids, whose sweeps are short, run far faster with many steps per launch;
 // large grids keep 8 (and the memory).
 static int default_steps_in_flight(long long plane, bool prec32) {
-  const long long per_step = plane * (5LL * (prec32 ? 4 : 8) + 1);
+  // per slot: FP32 a 32-byte record per cell, FP64 five 8-byte planes; a flag byte
+  const long long per_step = plane * ((prec32 ? 32LL : 5LL * 8) + 1);
   const long long k = per_step > 0 ? (1LL << 30) / per_step : FX_MAX_SLOTS - 1;
   return (int)std::max(8LL, std::min<long long>(FX_MAX_SLOTS - 1, k));
 }
@@ -335,14 +342,12 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
     const size_t pf = (size_t)d.plane * sizeof(float);
     float** fields[] = {&d.twet_f, &d.fe2_f, &d.fe3_f, &d.fn2_f, &d.fn3_f};
     float** pair_fields[] = {&d.eta, &d.eta_lo, &d.qx_f, &d.qy_f};
-    float** slot_fields[] = {&d.h_f, &d.h0_f, &d.hpm_f, &d.fe1_f, &d.fn1_f};
     if ((rc = dev_alloc(c, (void**)&d.zb, (size_t)d.plane * sizeof(double))) != FX_OK) goto fail;
     for (float** f : fields)
       if ((rc = dev_alloc(c, (void**)f, pf)) != FX_OK) goto fail;
     for (float** f : pair_fields)
       if ((rc = dev_alloc(c, (void**)f, 2 * pf)) != FX_OK) goto fail;
-    for (float** f : slot_fields)
-      if ((rc = dev_alloc(c, (void**)f, pf * d.nslot)) != FX_OK) goto fail;
+    if ((rc = dev_alloc(c, (void**)&d.rec32, (size_t)d.plane * d.nslot * 2 * sizeof(float4))) != FX_OK) goto fail;
     if ((rc = dev_alloc(c, (void**)&d.conc_f, pf * g->nchem)) != FX_OK) goto fail;
     if ((rc = dev_alloc(c, (void**)&c->stage, (size_t)d.plane * sizeof(double))) != FX_OK) goto fail;
     if ((rc = dev_alloc(c, (void**)&c->zstage, (size_t)d.plane * sizeof(double))) != FX_OK) goto fail;
@@ -443,8 +448,8 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
   const long long strips = (g->nrows + fx_ade_rows_per_strip() - 1) / fx_ade_rows_per_strip();
   const long long gx = (g->nrows + 30) / 31, gy = (g->ncols + 6) / 7;
   long long b = 0;
-  if (p->precision == 1)  // zb, twet and the flux fields, pairs, slots, solutes, extensions, 2 staging planes
-    b += plane * (8 + 5 * 4 + 4 * 2 * 4 + 5 * 4 * nslot + 4LL * g->nchem + 4LL * extension_grids + 16);
+  if (p->precision == 1)  // zb, twet and the flux fields, pairs, slot records, solutes, extensions, 2 staging planes
+    b += plane * (8 + 5 * 4 + 4 * 2 * 4 + 32 * nslot + 4LL * g->nchem + 4LL * extension_grids + 16);
   else
     b += plane * (6 * 8 + 3 * 2 * 8 + 5 * 8 * nslot + 8LL * g->nchem + 8LL * extension_grids);
   if (p->wintra && p->ade) b += plane * g->nchem * (p->precision == 1 ? 4 : 8);  // soil mass
@@ -468,6 +473,28 @@ __global__ void k_f64_to_f32(const double* __restrict__ src, float* __restrict__
 __global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__ dst, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] = (double)src[i];
+}
+// FP32 per-step field `comp` of the records from an FP64 plane: the current
+// slot's, and the ghost ring's in every slot. Nothing reads another slot's
+// interior before a step has written it (a step writes its slot's interior
+// records; the ADE sweep reads the slots of the steps it sweeps), while the
+// ghost ring is never written by a step.
+__global__ void k_rec_put(const __grid_constant__ fx_dev d, const double* __restrict__ src, int comp, int cur) {
+  float* rec = reinterpret_cast<float*>(d.rec32);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < d.plane;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float v = (float)src[i];
+    rec[8 * ((long long)cur * d.plane + i) + comp] = v;
+    const int icol = (int)(i / d.ld), irow = (int)(i - (long long)icol * d.ld) - FX_ROFF;
+    if (irow < 0 || irow > d.nr + 1) continue;  // padding
+    if (irow == 0 || irow == d.nr + 1 || icol == 0 || icol == d.nc + 1)
+      for (int k = 0; k < d.nslot; ++k)
+        if (k != cur) rec[8 * ((long long)k * d.plane + i) + comp] = v;
+  }
+}
+__global__ void k_rec_get(const float* __restrict__ rec, int comp, double* __restrict__ dst, long long plane) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (double)rec[8 * i + comp];
 }
 // z = zb + (eta + eta_lo) of the FP32 state (the order of get_z32's host sum before).
 __global__ void k_z_of_eta(const double* __restrict__ zb, const float* __restrict__ eta,
@@ -564,6 +591,16 @@ int fx_upload(fx_ctx* c, const char* field, const double* host) {
   } else {
     if (!strcmp(field, "soil_mass") && (rc = alloc_soil(c))) return rc;
     const FieldRef f = field_ref(c, field);
+    if (f.rec >= 0) {  // FP32 per-step field: one component of every slot's records
+      if ((rc = read_ctl(c))) return rc;
+      if ((rc = copy_in(c, c->stage, host))) return rc;
+      k_rec_put<<<plane_grid(c->d.plane), 256, 0, c->stream>>>(c->d, c->stage, f.rec,
+                                                               (int)(c->ctl_host->steps % c->d.nslot));
+      FX_CK(c, cudaGetLastError());
+      FX_CK(c, cudaStreamSynchronize(c->stream));
+      c->prepared = false;
+      return FX_OK;
+    }
     // Every plane of a slot or pair field holds the uploaded grid: the steps
     // overwrite the interior cells only, and the ghost ring they read stays
     // as uploaded. The host grid crosses PCIe once, into the current plane;
@@ -595,6 +632,16 @@ int fx_download(fx_ctx* c, const char* field, double* host) {
   const FieldRef f = field_ref(c, field);
   if (!f.ptr) {  // soil_mass never set
     std::fill(host, host + ((size_t)c->d.nr + 2) * ((size_t)c->d.nc + 2), 0.0);
+    return FX_OK;
+  }
+  if (f.rec >= 0) {  // FP32 per-step field: one component of the current slot's records
+    int rc = read_ctl(c);
+    if (rc) return rc;
+    k_rec_get<<<plane_grid(c->d.plane), 256, 0, c->stream>>>(
+        fx_rec(c->d, fx_slot(c->d, c->ctl_host->steps)), f.rec, c->stage, c->d.plane);
+    FX_CK(c, cudaGetLastError());
+    if ((rc = copy_out(c, host, c->stage))) return rc;
+    FX_CK(c, cudaStreamSynchronize(c->stream));
     return FX_OK;
   }
   const size_t esz = f.f32 ? sizeof(float) : sizeof(double);

@@ -144,9 +144,17 @@ struct fx_dev {
   int prec32;
   int ade_hold;  // failure-detection test: the ADE sweep's dependency waits are never satisfied
   float *eta, *eta_lo, *qx_f, *qy_f, *twet_f;
-  float *h_f, *h0_f, *hpm_f, *fe1_f, *fn1_f;  // nslot planes each
   float *fe2_f, *fe3_f, *fn2_f, *fn3_f;
   float* conc_f;                              // nchem planes
+  // FP32 state: the per-step fields (h, h0, the pre-melt depth hp, fe_1,
+  // fn_1) as one 32-byte record per cell and slot plane, {h0, h, hp, melt
+  // multiplier} then {fe_1, fn_1, flag byte (as the float's bits), 0}: the
+  // ADE sweep fetches a cell's step inputs as one sector instead of one
+  // sector per field (fx_ade.cu). The hydrodynamic step writes the record of
+  // each interior cell; the ghost ring holds what was uploaded. Cell gi of
+  // slot plane offset o is rec32[2 * (o + gi)], rec32[2 * (o + gi) + 1]
+  // (fx_rec). The flag byte is kept in the flags planes as well.
+  float4* rec32;
   const float* manning_f;
   const float* melt_mult_f;
   // ADE sweep scratch
@@ -213,6 +221,13 @@ __host__ __device__ inline void fx_dd_add(float& hi, float& lo, float x) {
   lo = t - (hi - s);
 }
 __host__ __device__ inline double fx_dd_val(float hi, float lo) { return (double)hi + (double)lo; }
+
+// Components of the FP32 state's per-step record (fx_dev::rec32).
+enum { FX_R_H0 = 0, FX_R_H = 1, FX_R_HP = 2, FX_R_MM = 3, FX_R_FE1 = 4, FX_R_FN1 = 5, FX_R_FL = 6 };
+// The record of the cell at slot-plane element o (slot offset + fx_ix).
+__host__ __device__ inline float* fx_rec(const fx_dev& d, long long o) {
+  return reinterpret_cast<float*>(d.rec32 + 2 * o);
+}
 
 // Offset of the plane of z (eta), qx, qy that holds the state after step n:
 // these fields have two planes, so a step reads one while it writes the

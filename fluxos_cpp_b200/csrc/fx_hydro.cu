@@ -923,6 +923,14 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
   out[5] = fn3;
 }
 
+// The per-step record of an owned cell in the step's slot (fx_dev::rec32).
+__device__ __forceinline__ void put_rec32(const fx_dev& d, long long o, float h0, float h, float hp, float mm,
+                                          float fe1, float fn1, uint8_t fl) {
+  float4* r = d.rec32 + 2 * o;
+  r[0] = make_float4(h0, h, hp, mm);
+  r[1] = make_float4(fe1, fn1, __uint_as_float((unsigned)fl), 0.0f);
+}
+
 template <int BY>
 __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
                                              HydroSmem32<BY>& S, TilePart& acc, const unsigned char* stg = nullptr) {
@@ -954,7 +962,6 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       if (melt_on && !(fl & FX_F_NODATA)) {
         const float mi = melt32(d, c, d.melt_mult_f ? d.melt_mult_f[gi] : 1.0f);
         bmelt = (double)mi * d.arbase;
-        if (d.ade) d.hpm_f[scur + gi] = hpre;
         fx_dd_add(eta1, lo1, mi);
         h1 = fmaxf(eta1, 0.0f);
         depth = fx_dd_val(eta1, lo1);
@@ -974,13 +981,13 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       d.eta_lo[pcur + gi] = lo1;
       d.qx_f[pcur + gi] = qx;
       d.qy_f[pcur + gi] = qy;
-      d.h_f[scur + gi] = h1;
-      d.h0_f[scur + gi] = h1;
-      d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
-      if (scur != sprev) {
-        d.fe1_f[scur + gi] = d.fe1_f[sprev + gi];
-        d.fn1_f[scur + gi] = d.fn1_f[sprev + gi];
-      }
+      const uint8_t fl1 = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+      d.flags[scur + gi] = fl1;
+      // fluxes are unchanged by a step without solver
+      const float* rp = fx_rec(d, sprev + gi);
+      const bool melted = melt_on && !(fl & FX_F_NODATA);
+      put_rec32(d, scur + gi, h1, h1, melted ? hpre : 0.0f, melted && d.melt_mult_f ? d.melt_mult_f[gi] : 1.0f,
+                rp[FX_R_FE1], rp[FX_R_FN1], fl1);
       courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
     }
     acc.add(dtc, hm, bmelt, 0.0);
@@ -1084,10 +1091,11 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
                           (S.cls[sidx(sr, scc - 1)] & C_DRY) && (S.cls[sidx(sr, scc + 1)] & C_DRY);
       if (alldry) {  // all five cells dry: the last computed fluxes stay (solver_drydomain.cpp:60-76)
         const long long gi = fx_ix(d, irow0 - 1 + fr, icol0 - 1 + fc);
-        S.f[0][k] = d.fe1_f[sprev + gi];
+        const float* rp = fx_rec(d, sprev + gi);
+        S.f[0][k] = rp[FX_R_FE1];
         S.f[1][k] = d.fe2_f[gi];
         S.f[2][k] = d.fe3_f[gi];
-        S.f[3][k] = d.fn1_f[sprev + gi];
+        S.f[3][k] = rp[FX_R_FN1];
         S.f[4][k] = d.fn2_f[gi];
         S.f[5][k] = d.fn3_f[gi];
       } else {
@@ -1112,11 +1120,13 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     const float etapre = stg ? reinterpret_cast<const float*>(stg + L::O_Z)[i4] : d.eta[pprev + gi];
     float h0v = fmaxf(0.0f, etapre);
     double mi = 0.0;
+    float hpv = 0.0f, mmv = 1.0f;  // the ADE record's pre-melt depth and melt multiplier
     if (melt_on && !(fl & FX_F_NODATA)) {
       h0v = fmaxf(eta1, 0.0f);
-      if (d.ade) d.hpm_f[scur + gi] = fmaxf(etapre, 0.0f);
+      hpv = fmaxf(etapre, 0.0f);
       const float mm = !d.melt_mult_f ? 1.0f
                        : (stg ? reinterpret_cast<const float*>(stg + L::O_MM)[i4] : d.melt_mult_f[gi]);
+      mmv = mm;
       mi = (double)melt32(d, c, mm);
       bmelt = mi * d.arbase;
     }
@@ -1171,27 +1181,25 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     }
     d.eta[pcur + gi] = eta;
     d.eta_lo[pcur + gi] = lo;
-    d.h_f[scur + gi] = h;
     d.qx_f[pcur + gi] = qx;
     d.qy_f[pcur + gi] = qy;
-    d.h0_f[scur + gi] = h0v;
-    d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+    const uint8_t fl1 = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+    d.flags[scur + gi] = fl1;
+    float fe1v = 0.0f, fn1v = 0.0f;
     if ((cl & C_INT) && !wall) {
       const bool computed =
           !(cl & C_DRY) || !((S.cls[sidx(lx + 1, ly + 2)] & C_DRY) && (S.cls[sidx(lx + 3, ly + 2)] & C_DRY) &&
                              (S.cls[sidx(lx + 2, ly + 1)] & C_DRY) && (S.cls[sidx(lx + 2, ly + 3)] & C_DRY));
-      d.fe1_f[scur + gi] = S.f[0][fP];
-      d.fn1_f[scur + gi] = S.f[3][fP];
+      fe1v = S.f[0][fP];
+      fn1v = S.f[3][fP];
       if (computed && (d.store_all_fluxes || !(depth > d.hdry))) {
         d.fe2_f[gi] = S.f[1][fP];
         d.fe3_f[gi] = S.f[2][fP];
         d.fn2_f[gi] = S.f[4][fP];
         d.fn3_f[gi] = S.f[5][fP];
       }
-    } else if (scur != sprev) {
-      d.fe1_f[scur + gi] = 0.0f;
-      d.fn1_f[scur + gi] = 0.0f;
     }
+    put_rec32(d, scur + gi, h0v, h, hpv, mmv, fe1v, fn1v, fl1);
     courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
   }
   acc.add(dtc, hm, bmelt, bout);
@@ -2024,7 +2032,7 @@ __global__ void __launch_bounds__(256) k_mass(const __grid_constant__ fx_dev d, 
     const int icol = (int)(i / d.ld), irow = (int)(i % d.ld) - FX_ROFF;
     if (irow < 1 || irow > d.nr || icol < 1 || icol > d.nc) continue;
     if (d.flags[sl + i] & FX_F_WALL) continue;
-    const double h = d.prec32 ? (double)d.h_f[sl + i] : d.h[sl + i];
+    const double h = d.prec32 ? (double)fx_rec(d, sl + i)[FX_R_H] : d.h[sl + i];
     acc[0] += d.prec32 ? fx_dd_val(d.eta[pl + i], d.eta_lo[pl + i]) : d.z[pl + i] - d.zb[i];
     for (int k = 0; k < d.nchem; ++k)
       acc[1 + k] += h * (d.prec32 ? (double)d.conc_f[k * d.plane + i] : d.conc[k * d.plane + i]);

@@ -19,7 +19,7 @@ namespace fxres {
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ double cell_h(const fx_dev& d, long long sl, long long gi) {
-  return d.prec32 ? (double)d.h_f[sl + gi] : d.h[sl + gi];
+  return d.prec32 ? (double)fx_rec(d, sl + gi)[FX_R_H] : d.h[sl + gi];
 }
 
 __device__ __forceinline__ bool selected(const fx_dev& d, long long sl, long long gi, double hmin) {
@@ -113,8 +113,8 @@ __global__ void k_write(const __grid_constant__ fx_dev d, double hmin, const lon
           qy = (double)d.qy_f[pp + gi];
           conc = (double)d.conc_f[gi];
           soil = d.soil_f ? (double)d.soil_f[gi] : 0.0;
-          fe1 = (double)d.fe1_f[sl + gi];
-          fn1 = (double)d.fn1_f[sl + gi];
+          fe1 = (double)fx_rec(d, sl + gi)[FX_R_FE1];
+          fn1 = (double)fx_rec(d, sl + gi)[FX_R_FN1];
           twet = (double)d.twet_f[gi];
         } else {
           z = d.z[pp + gi];
