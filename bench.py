@@ -604,8 +604,8 @@ def run_mix(args, peak: float) -> dict:
     steps = args.mix_steps
 
     def batch_rate(precision, match_steps=None):
-        # FP32 members hold 63 steps in flight (82 GB for the 64 scenarios); FP64 ones
-        # args.mix_in_flight (memory: FP64 slot planes are twice as large)
+        # FP32 members hold 63 steps in flight (about 130 GB for the 64 scenarios: a
+        # 33-byte slot record per cell and step); FP64 ones args.mix_in_flight (41 bytes)
         from fluxos_cpp_b200 import accuracy as A
         k_members = 63 if precision == "fp32" else args.mix_in_flight
         doms = [S.make_domain(sc, precision=precision, steps_in_flight=k_members) for sc in scs]

@@ -98,6 +98,11 @@ class Server:
         self.clock = clock
         self.pool = cf.ThreadPoolExecutor(max_workers=host_threads)
         self.lookahead = host_threads
+        # retired domains are released on their own thread (freeing device
+        # memory waits for the device), so the loop goes on stepping; their
+        # bytes count against the cap until the release has finished
+        self.closer = cf.ThreadPoolExecutor(max_workers=1)
+        self.closing: List[tuple] = []  # (future, bytes)
         self.batch = (batch_factory or fx.Batch)()
         self.make_domain = make_domain or S.make_domain
         self.active: List[tuple] = []  # (request, domain, bytes)
@@ -106,13 +111,28 @@ class Server:
         self.peak_members = 0
         self.cell_updates = 0
         self.gpu_busy = 0.0
+        # host time of the request loop outside the batch steps, by part
+        self.host_s = {"admit": 0.0, "retire": 0.0, "status": 0.0, "idle": 0.0}
 
     def close(self) -> None:
         for _, d, _ in self.active:
             d.close()
         self.active = []
+        self._released(wait=True)
         self.batch.close()
         self.pool.shutdown(wait=False)
+        self.closer.shutdown(wait=True)
+
+    def _released(self, wait: bool = False) -> None:
+        """Drop finished releases of retired domains from the memory count."""
+        keep = []
+        for f, nbytes in self.closing:
+            if wait or f.done():
+                f.result()
+                self.used -= nbytes
+            else:
+                keep.append((f, nbytes))
+        self.closing = keep
 
     @staticmethod
     def footprint(r: Request) -> int:
@@ -127,8 +147,7 @@ class Server:
         r.water = d.mass()[0]
         for k in self.keep:
             r.state[k] = d.download(k)
-        d.close()
-        self.used -= nbytes
+        self.closing.append((self.closer.submit(d.close), nbytes))
         r.done = now
 
     def _prepare(self, r: Request, t0: float, gen: Optional[cf.Future] = None):
@@ -172,6 +191,7 @@ class Server:
             r.inputs = r.make()
 
         while pending or preparing or self.active:
+            self._released()
             now = self.clock() - t0
             # the look-ahead generator: inputs of requests arriving within generate_ahead
             while to_generate and to_generate[0].arrival <= now + generate_ahead and \
@@ -199,6 +219,7 @@ class Server:
                 reserved += need
                 pending.popleft()
             # admit finished preparations
+            ta = self.clock()
             for rid in [k for k, (_, f, _) in preparing.items() if f.done()]:
                 r, f, need = preparing.pop(rid)
                 reserved -= need
@@ -210,11 +231,16 @@ class Server:
                 self.peak_used = max(self.peak_used, self.used + reserved)
                 self.peak_members = max(self.peak_members, len(self.active))
                 r.admitted = self.clock() - t0
+            self.host_s["admit"] += self.clock() - ta
             if not self.active:
+                ti = self.clock()
                 time.sleep(0.001)
+                self.host_s["idle"] += self.clock() - ti
                 continue
+            ts = self.clock()
             before = [d.status()["steps"] for _, d, _ in self.active]
             g0 = self.clock()
+            self.host_s["status"] += g0 - ts
             sts = self.batch.step(self.chunk)
             self.gpu_busy += self.clock() - g0
             now = self.clock() - t0
@@ -230,14 +256,17 @@ class Server:
                         self.on_output(r, d)
                     d.print_done()
                 if st["finished"]:
+                    tr = self.clock()
                     self._retire(i, now)
+                    self.host_s["retire"] += self.clock() - tr
         wall = self.clock() - t0
+        self._released(wait=True)
         if gen_pool is not None:
             gen_pool.shutdown(wait=True)
         part = {"records": [record(r) for r in requests], "wall_s": wall, "cell_updates": self.cell_updates,
                 "inputs_late": late_inputs if gen_pool is not None else None,
                 "peak_device_bytes": self.peak_used, "peak_members": self.peak_members,
-                "batch_step_s": self.gpu_busy}
+                "batch_step_s": self.gpu_busy, "host_s": dict(self.host_s)}
         self.last_part = part  # this server's records, for merging with other ranks' (summarize)
         return summarize([part])
 
@@ -282,7 +311,9 @@ def summarize(parts: List[dict]) -> dict:
             "inputs_late": sum(late) if late else None,
             "peak_device_bytes": max(p["peak_device_bytes"] for p in parts),
             "peak_members": max(p["peak_members"] for p in parts),
-            "batch_step_s": max(p["batch_step_s"] for p in parts)}
+            "batch_step_s": max(p["batch_step_s"] for p in parts),
+            "host_s": {k: max(p.get("host_s", {}).get(k, 0.0) for p in parts)
+                       for k in ("admit", "retire", "status", "idle")}}
 
 
 def shard(requests: List[Request], rank: int, world: int) -> List[Request]:
