@@ -80,10 +80,12 @@ ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
 # (dram__bytes_read.sum + dram__bytes_write.sum from ncu on the 2048 x 2048
 # case of this workload, one launch, divided by the cells and the steps the
 # launch covers: profiles/k_ade_one_fractal2048.md,
-# profiles/k_hydro_tma_fractal2048.md); traffic scales with the cells, so
-# `traffic` in the line is this times the cells of the run.
-DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 143.32, "k_ade_sweep": 49.33},
-                       "fp32": {"k_hydro": 80.45, "k_ade_sweep": 23.66}}
+# profiles/k_hydro_tma_fractal2048.md; the FP32 hydrodynamic kernel with
+# 16-row tiles, the FP64 one with 8-row tiles, the shapes the autotuner
+# picks); traffic scales with the cells, so `traffic` in the line is this
+# times the cells of the run.
+DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 143.32, "k_ade_sweep": 47.47},
+                       "fp32": {"k_hydro": 91.45, "k_ade_sweep": 34.60}}
 
 
 def _rank():
