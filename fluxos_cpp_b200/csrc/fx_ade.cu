@@ -60,19 +60,21 @@ constexpr long long HOLD_SPIN_LIMIT = 1LL << 12;  // the same with fx_dev.ade_ho
 // T is the state's precision (double for the reference path, float for the
 // single-precision state).
 template <class T>
-struct Ring {
-  static constexpr int CV = 16 / sizeof(T);  // values per 16-byte copy
+struct Ring;
+// The FP64 ring: the concentration group, the cell's six per-step values
+// {h0, h, hp, fe_1, fn_1, flag bits} and the melt multiplier. A context's
+// record (fx_dev::rec64) lands in r as three 16-byte copies; the separate
+// arrays of fx_adesolver_noalloc land in the same places one by one (the
+// flag as the 4-byte word holding it, in r[5]'s low half).
+template <>
+struct Ring<double> {
+  static constexpr int CV = 2;
   // the 16-byte aligned group of concentrations holding this lane's cell: it
   // is written during the launch by other warps, so it is copied with
   // cp.async.cg (L2 only; L1 is not coherent across SMs), which moves 16 bytes
-  T c[RING][32][CV];
-  T h0[RING][32];   // depth after the melt, before the update
-  T h[RING][32];    // depth after the update
-  T hp[RING][32];   // depth before the step's melt
-  T mm[RING][32];   // melt-rate multiplier (1 without a melt field)
-  T fe1[RING][32];  // fe_1
-  T fn1[RING][32];  // fn_1
-  unsigned fl[RING][32]; // the 4-byte word holding the cell's flag byte
+  double c[RING][32][CV];
+  double r[RING][32][FX_R64_N];
+  double mm[RING][32];  // melt-rate multiplier (1 without a melt field)
 };
 
 // The FP32 state's ring: the concentration group and the cell's per-step
@@ -102,7 +104,6 @@ template <>
 struct Fields<double> {
   static __device__ __forceinline__ const double* h(const fx_dev& d) { return d.h; }
   static __device__ __forceinline__ const double* h0(const fx_dev& d) { return d.h0; }
-  static __device__ __forceinline__ const double* hpm(const fx_dev& d) { return d.hpm; }
   static __device__ __forceinline__ const double* fe1(const fx_dev& d) { return d.fe1; }
   static __device__ __forceinline__ const double* fn1(const fx_dev& d) { return d.fn1; }
   static __device__ __forceinline__ const double* mm(const fx_dev& d) { return d.melt_mult; }
@@ -193,18 +194,23 @@ __device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const
                      (unsigned)__cvta_generic_to_shared(&R.b[slot][lane])),
                  "l"(rec + 1), "r"(inr ? 16 : 0));
   } else {
-    const int nb = inr ? B : 0;
-    const unsigned e = (unsigned)__cvta_generic_to_shared(&R) + (unsigned)(slot * 32 + lane) * B;
-    cp_async_sz(e + (unsigned)offsetof(Ring<T>, h0), F::h0(d) + o, nb, B);
-    cp_async_sz(e + (unsigned)offsetof(Ring<T>, h), F::h(d) + o, nb, B);
-    const bool dil = S.dilute;
-    cp_async_sz(e + (unsigned)offsetof(Ring<T>, hp), dil ? F::hpm(d) + o : F::h(d), dil ? nb : 0, B);
-    const bool mm_ok = dil && F::mm(d) != nullptr;
-    cp_async_sz(e + (unsigned)offsetof(Ring<T>, mm), mm_ok ? F::mm(d) + gi : F::h(d), mm_ok ? nb : 0, B);
-    cp_async_sz(e + (unsigned)offsetof(Ring<T>, fe1), F::fe1(d) + o, nb, B);
-    cp_async_sz(e + (unsigned)offsetof(Ring<T>, fn1), F::fn1(d) + o, nb, B);
-    // the 4-byte word holding the flag byte (slot planes are multiples of 32 bytes)
-    cp_async_sz((unsigned)__cvta_generic_to_shared(&R.fl[slot][lane]), d.flags + (o & ~3LL), inr ? 4 : 0, 4);
+    double* re = &R.r[slot][lane][0];
+    const unsigned e = (unsigned)__cvta_generic_to_shared(re);
+    if (d.rec64) {  // a context: the cell's record, 48 bytes
+      const double* rec = fx_rec64(d, o);
+      for (int q = 0; q < 3; ++q) cp_async_sz(e + 16 * q, rec + 2 * q, inr ? 16 : 0, 16);
+    } else {  // fx_adesolver_noalloc: the caller's arrays (no melt, no slots)
+      const int nb = inr ? 8 : 0;
+      cp_async_sz(e + 8 * FX_R64_H0, F::h0(d) + o, nb, 8);
+      cp_async_sz(e + 8 * FX_R64_H, F::h(d) + o, nb, 8);
+      cp_async_sz(e + 8 * FX_R64_FE1, F::fe1(d) + o, nb, 8);
+      cp_async_sz(e + 8 * FX_R64_FN1, F::fn1(d) + o, nb, 8);
+      // the 4-byte word holding the flag byte (planes are multiples of 32 bytes)
+      cp_async_sz(e + 8 * FX_R64_FL, d.flags + (o & ~3LL), inr ? 4 : 0, 4);
+    }
+    const bool mm_ok = S.dilute && F::mm(d) != nullptr;
+    cp_async_sz((unsigned)__cvta_generic_to_shared(&R.mm[slot][lane]),
+                mm_ok ? (const void*)(F::mm(d) + gi) : (const void*)d.flags, mm_ok && inr ? 8 : 0, 8);
   }
 }
 
@@ -214,6 +220,7 @@ __device__ __forceinline__ void prefetch(const fx_dev& d, const StepIn& S, const
 template <class T>
 __device__ __forceinline__ Rec<T> make_rec_br(const fx_dev& d, const StepIn& S, const Ring<T>& R, int lane, int ix,
                                            int iy) {
+  static_assert(sizeof(T) == 8, "the branch form reads the FP64 ring");
   Rec<T> r;
   r.c = T(0);
   r.b = T(0);
@@ -223,28 +230,28 @@ __device__ __forceinline__ Rec<T> make_rec_br(const fx_dev& d, const StepIn& S, 
   r.ld = 0;
   if (ix < 0 || ix > d.nr + 1 || iy < 0 || iy > d.nc + 1) return r;
   const int slot = iy & (RING - 1);
-  r.h = R.h[slot][lane];
+  const double* v = R.r[slot][lane];
+  r.h = v[FX_R64_H];
   if (ix >= 1 && ix <= d.nr && iy >= 1 && iy <= d.nc) {
     const long long gi = fx_ix(d, ix, iy);
-    const unsigned fl = (R.fl[slot][lane] >> (8 * (unsigned)(gi & 3))) & 0xffu;
+    // a record holds the flag byte itself, a separate flags array the word holding it
+    const unsigned word = (unsigned)__double_as_longlong(v[FX_R64_FL]);
+    const unsigned fl = (d.rec64 ? word : word >> (8 * (unsigned)(gi & 3))) & 0xffu;
     r.ld = fl & FX_F_LDRY;
     const int ldp = (fl & FX_F_LDRY_PREV) ? 1 : 0;
     T c = R.c[slot][lane][gi & (Ring<T>::CV - 1)];
-    const T h0 = R.h0[slot][lane];
+    const T h0 = v[FX_R64_H0];
     // the inflow cell holds h0 only after its inflow; the melt's dilution
     // divides by the depth after the melt (common.cpp:226-234, 313-325)
     const bool inflow_cell = gi == S.inflow_gi;
     const T hm = inflow_cell ? (T)S.inflow_hm : h0;
     if (S.dilute && !(fl & FX_F_NODATA)) {
-      const T hp = R.hp[slot][lane];
+      const T hp = v[FX_R64_HP];
       if (hp != T(0)) {
-        // the melt depth the hydrodynamic step added (FP32 state: melt32 in fx_hydro.cu)
-        T mi;
-        if constexpr (sizeof(T) == 4)
-          mi = Fields<T>::mm(d) ? (T)(S.meteoi * (double)R.mm[slot][lane]) : (T)S.meteoi;
-        else
-          mi = Fields<T>::mm(d) ? (T)((double)S.meteo_rate * (double)R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
-                                : (T)S.meteoi;
+        // the melt depth the hydrodynamic step added (melt_depth in fx_hydro.cu)
+        const T mi = Fields<T>::mm(d)
+                         ? (T)((double)S.meteo_rate * R.mm[slot][lane] / (1000. * 3600. * 24.) * S.dt)
+                         : (T)S.meteoi;
         c = tdiv(c * hp + (mi * (T)S.mconc), hm);
       }
     }
@@ -254,8 +261,8 @@ __device__ __forceinline__ Rec<T> make_rec_br(const fx_dev& d, const StepIn& S, 
     else if (r.ld == 0 && ldp == 0) r.b = tdiv(c * h0, r.h);
     else if (r.ld == 1) r.b = T(0);
     else r.b = c;
-    r.qx = R.fe1[slot][lane];
-    r.qy = R.fn1[slot][lane];
+    r.qx = v[FX_R64_FE1];
+    r.qy = v[FX_R64_FN1];
   }
   return r;
 }

@@ -48,7 +48,7 @@ struct FieldRef {
   bool slot = false;  // one plane per slot
   bool pair = false;  // two planes, the current one is fx_pp(steps)
   int copies = 1;     // identical planes (the soil mass: one per solute)
-  int rec = -1;       // FP32 per-step field: its component of the slot records (FX_R_*)
+  int rec = -1;       // per-step field: its component of the slot records (FX_R64_* or FX_R_*)
 };
 
 static FieldRef field_ref(fx_ctx* c, const char* name) {
@@ -61,23 +61,23 @@ static FieldRef field_ref(fx_ctx* c, const char* name) {
     r.slot = slot;
     r.pair = pair;
   };
-  // a per-step field: FP64 slot planes, or a component of the FP32 slot records
-  auto pick_rec = [&](void* p64, int comp) {
-    pick(p64, d.rec32, true);
-    if (p32) r.rec = comp;
+  // a per-step field: a component of the slot records (FP64 rec64, FP32 rec32)
+  auto pick_rec = [&](int comp64, int comp32) {
+    pick(d.rec64, d.rec32, true);
+    r.rec = p32 ? comp32 : comp64;
   };
   if (!strcmp(name, "zb")) r.ptr = d.zb;  // FP64 in both forms
   else if (!strcmp(name, "z")) {
     if (!p32) pick(d.z, nullptr, false, true);  // FP32: held as eta, see fx_upload / fx_download
-  } else if (!strcmp(name, "h")) pick_rec(d.h, FX_R_H);
+  } else if (!strcmp(name, "h")) pick_rec(FX_R64_H, FX_R_H);
   else if (!strcmp(name, "qx")) pick(d.qx, d.qx_f, false, true);
   else if (!strcmp(name, "qy")) pick(d.qy, d.qy_f, false, true);
   else if (!strcmp(name, "twet")) pick(d.twet, d.twet_f, false);
-  else if (!strcmp(name, "h0")) pick_rec(d.h0, FX_R_H0);
-  else if (!strcmp(name, "fe_1")) pick_rec(d.fe1, FX_R_FE1);
+  else if (!strcmp(name, "h0")) pick_rec(FX_R64_H0, FX_R_H0);
+  else if (!strcmp(name, "fe_1")) pick_rec(FX_R64_FE1, FX_R_FE1);
   else if (!strcmp(name, "fe_2")) pick(d.fe2, d.fe2_f, false);
   else if (!strcmp(name, "fe_3")) pick(d.fe3, d.fe3_f, false);
-  else if (!strcmp(name, "fn_1")) pick_rec(d.fn1, FX_R_FN1);
+  else if (!strcmp(name, "fn_1")) pick_rec(FX_R64_FN1, FX_R_FN1);
   else if (!strcmp(name, "fn_2")) pick(d.fn2, d.fn2_f, false);
   else if (!strcmp(name, "fn_3")) pick(d.fn3, d.fn3_f, false);
   else if (!strncmp(name, "conc", 4)) {
@@ -265,8 +265,8 @@ const char* fx_last_error(const fx_ctx* ctx) { return ctx ? ctx->err.c_str() : g
 // grids, whose sweeps are short, run far faster with many steps per launch;
 // large grids keep 8 (and the memory).
 static int default_steps_in_flight(long long plane, bool prec32) {
-  // per slot: FP32 a 32-byte record per cell, FP64 five 8-byte planes; a flag byte
-  const long long per_step = plane * ((prec32 ? 32LL : 5LL * 8) + 1);
+  // per slot: a 32-byte (FP32) or 48-byte (FP64) record per cell, and a flag byte
+  const long long per_step = plane * ((prec32 ? 32LL : 48LL) + 1);
   const long long k = per_step > 0 ? (1LL << 30) / per_step : FX_MAX_SLOTS - 1;
   return (int)std::max(8LL, std::min<long long>(FX_MAX_SLOTS - 1, k));
 }
@@ -330,13 +330,13 @@ int fx_create(const fx_grid* g, const fx_params* p, fx_ctx** out) {
     const size_t pb = (size_t)d.plane * sizeof(double);
     double** fields[] = {&d.zb, &d.twet, &d.fe2, &d.fe3, &d.fn2, &d.fn3};
     double** pair_fields[] = {&d.z, &d.qx, &d.qy};
-    double** slot_fields[] = {&d.h, &d.h0, &d.hpm, &d.fe1, &d.fn1};
     for (double** f : fields)
       if ((rc = dev_alloc(c, (void**)f, pb)) != FX_OK) goto fail;
     for (double** f : pair_fields)
       if ((rc = dev_alloc(c, (void**)f, 2 * pb)) != FX_OK) goto fail;
-    for (double** f : slot_fields)
-      if ((rc = dev_alloc(c, (void**)f, pb * d.nslot)) != FX_OK) goto fail;
+    if ((rc = dev_alloc(c, (void**)&d.rec64, pb * FX_R64_N * d.nslot)) != FX_OK) goto fail;
+    // staging plane of the per-step fields' uploads and downloads
+    if ((rc = dev_alloc(c, (void**)&c->stage, pb)) != FX_OK) goto fail;
     if ((rc = dev_alloc(c, (void**)&d.conc, pb * g->nchem)) != FX_OK) goto fail;
   } else {
     const size_t pf = (size_t)d.plane * sizeof(float);
@@ -451,7 +451,7 @@ int fx_footprint(const fx_grid* g, const fx_params* p, int extension_grids, long
   if (p->precision == 1)  // zb, twet and the flux fields, pairs, slot records, solutes, extensions, 2 staging planes
     b += plane * (8 + 5 * 4 + 4 * 2 * 4 + 32 * nslot + 4LL * g->nchem + 4LL * extension_grids + 16);
   else
-    b += plane * (6 * 8 + 3 * 2 * 8 + 5 * 8 * nslot + 8LL * g->nchem + 8LL * extension_grids);
+    b += plane * (6 * 8 + 3 * 2 * 8 + 48 * nslot + 8LL * g->nchem + 8LL * extension_grids + 8);  // + staging
   if (p->wintra && p->ade) b += plane * g->nchem * (p->precision == 1 ? 4 : 8);  // soil mass
   b += plane * nslot;                                   // flags
   b += (long long)sizeof(fx_ctl) + 3 * FX_METEO_ROWS * 4 + (long long)sizeof(fx_dev);
@@ -474,28 +474,33 @@ __global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] = (double)src[i];
 }
-// FP32 per-step field `comp` of the records from an FP64 plane: the current
+// Per-step field `comp` of the slot records (R = float: rec32, 8 floats a
+// cell; R = double: rec64, 6 doubles a cell) from an FP64 plane: the current
 // slot's, and the ghost ring's in every slot. Nothing reads another slot's
 // interior before a step has written it (a step writes its slot's interior
 // records; the ADE sweep reads the slots of the steps it sweeps), while the
 // ghost ring is never written by a step.
-__global__ void k_rec_put(const __grid_constant__ fx_dev d, const double* __restrict__ src, int comp, int cur) {
-  float* rec = reinterpret_cast<float*>(d.rec32);
+extern "C++" {
+template <class R, int N>
+__global__ void k_rec_put(const __grid_constant__ fx_dev d, R* __restrict__ rec, const double* __restrict__ src,
+                          int comp, int cur) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < d.plane;
        i += (long long)gridDim.x * blockDim.x) {
-    const float v = (float)src[i];
-    rec[8 * ((long long)cur * d.plane + i) + comp] = v;
+    const R v = (R)src[i];
+    rec[N * ((long long)cur * d.plane + i) + comp] = v;
     const int icol = (int)(i / d.ld), irow = (int)(i - (long long)icol * d.ld) - FX_ROFF;
     if (irow < 0 || irow > d.nr + 1) continue;  // padding
     if (irow == 0 || irow == d.nr + 1 || icol == 0 || icol == d.nc + 1)
       for (int k = 0; k < d.nslot; ++k)
-        if (k != cur) rec[8 * ((long long)k * d.plane + i) + comp] = v;
+        if (k != cur) rec[N * ((long long)k * d.plane + i) + comp] = v;
   }
 }
-__global__ void k_rec_get(const float* __restrict__ rec, int comp, double* __restrict__ dst, long long plane) {
+template <class R, int N>
+__global__ void k_rec_get(const R* __restrict__ rec, int comp, double* __restrict__ dst, long long plane) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x)
-    dst[i] = (double)rec[8 * i + comp];
+    dst[i] = (double)rec[N * i + comp];
 }
+}  // extern "C++"
 // z = zb + (eta + eta_lo) of the FP32 state (the order of get_z32's host sum before).
 __global__ void k_z_of_eta(const double* __restrict__ zb, const float* __restrict__ eta,
                            const float* __restrict__ lo, double* __restrict__ z, long long n) {
@@ -594,8 +599,13 @@ int fx_upload(fx_ctx* c, const char* field, const double* host) {
     if (f.rec >= 0) {  // FP32 per-step field: one component of every slot's records
       if ((rc = read_ctl(c))) return rc;
       if ((rc = copy_in(c, c->stage, host))) return rc;
-      k_rec_put<<<plane_grid(c->d.plane), 256, 0, c->stream>>>(c->d, c->stage, f.rec,
-                                                               (int)(c->ctl_host->steps % c->d.nslot));
+      const int cur = (int)(c->ctl_host->steps % c->d.nslot);
+      if (c->d.prec32)
+        k_rec_put<float, 8><<<plane_grid(c->d.plane), 256, 0, c->stream>>>(
+            c->d, reinterpret_cast<float*>(c->d.rec32), c->stage, f.rec, cur);
+      else
+        k_rec_put<double, FX_R64_N><<<plane_grid(c->d.plane), 256, 0, c->stream>>>(c->d, c->d.rec64, c->stage,
+                                                                                   f.rec, cur);
       FX_CK(c, cudaGetLastError());
       FX_CK(c, cudaStreamSynchronize(c->stream));
       c->prepared = false;
@@ -637,8 +647,13 @@ int fx_download(fx_ctx* c, const char* field, double* host) {
   if (f.rec >= 0) {  // FP32 per-step field: one component of the current slot's records
     int rc = read_ctl(c);
     if (rc) return rc;
-    k_rec_get<<<plane_grid(c->d.plane), 256, 0, c->stream>>>(
-        fx_rec(c->d, fx_slot(c->d, c->ctl_host->steps)), f.rec, c->stage, c->d.plane);
+    const long long o = fx_slot(c->d, c->ctl_host->steps);
+    if (c->d.prec32)
+      k_rec_get<float, 8><<<plane_grid(c->d.plane), 256, 0, c->stream>>>(fx_rec(c->d, o), f.rec, c->stage,
+                                                                        c->d.plane);
+    else
+      k_rec_get<double, FX_R64_N><<<plane_grid(c->d.plane), 256, 0, c->stream>>>(fx_rec64(c->d, o), f.rec,
+                                                                                c->stage, c->d.plane);
     FX_CK(c, cudaGetLastError());
     if ((rc = copy_out(c, host, c->stage))) return rc;
     FX_CK(c, cudaStreamSynchronize(c->stream));

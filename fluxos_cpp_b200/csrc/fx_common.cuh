@@ -111,9 +111,18 @@ struct fx_dev {
   // plane n & 1 (fx_pp).
   int nslot;
   int wintra;         // WINTRA soil release after each step's ADE sweep (needs ade)
-  double *z, *zb, *h, *qx, *qy, *twet, *h0;
-  double* hpm;        // per slot: the depth before the step's melt, max(z - zb, 0) (common.cpp:216)
-  double *fe1, *fe2, *fe3, *fn1, *fn2, *fn3;
+  double *z, *zb, *qx, *qy, *twet;
+  // FP64 per-step fields of a context: one 48-byte record per cell and slot
+  // plane, {h0, h, hp (the depth before the step's melt, max(z - zb, 0),
+  // common.cpp:216), fe_1, fn_1, flag byte (as the double's bits)}, read by
+  // the ADE sweep as three 16-byte copies (fx_rec64). The hydrodynamic step
+  // writes the record of each interior cell; the ghost ring holds what was
+  // uploaded.
+  double* rec64;
+  // The same fields as separate arrays: set (and rec64 left null) only by
+  // fx_adesolver_noalloc, whose caller owns them.
+  double *h, *h0, *fe1, *fn1;
+  double *fe2, *fe3, *fn2, *fn3;
   double* conc;       // nchem planes of ld*(nc+2)
   uint8_t* flags;
   // extensions (nullptr = off)
@@ -228,6 +237,9 @@ enum { FX_R_H0 = 0, FX_R_H = 1, FX_R_HP = 2, FX_R_MM = 3, FX_R_FE1 = 4, FX_R_FN1
 __host__ __device__ inline float* fx_rec(const fx_dev& d, long long o) {
   return reinterpret_cast<float*>(d.rec32 + 2 * o);
 }
+// Components of the FP64 per-step record (fx_dev::rec64), 6 doubles a cell.
+enum { FX_R64_H0 = 0, FX_R64_H = 1, FX_R64_HP = 2, FX_R64_FE1 = 3, FX_R64_FN1 = 4, FX_R64_FL = 5, FX_R64_N = 6 };
+__host__ __device__ inline double* fx_rec64(const fx_dev& d, long long o) { return d.rec64 + FX_R64_N * o; }
 
 // Offset of the plane of z (eta), qx, qy that holds the state after step n:
 // these fields have two planes, so a step reads one while it writes the

@@ -923,6 +923,16 @@ __device__ void solver_dry32(const fx_dev& d, const SM& S, int sr, int sc, int i
   out[5] = fn3;
 }
 
+// The FP64 per-step record of an owned cell in the step's slot
+// (fx_dev::rec64), as three 16-byte stores.
+__device__ __forceinline__ void put_rec64(const fx_dev& d, long long o, double h0, double h, double hp, double fe1,
+                                          double fn1, uint8_t fl) {
+  double2* r = reinterpret_cast<double2*>(fx_rec64(d, o));
+  r[0] = make_double2(h0, h);
+  r[1] = make_double2(hp, fe1);
+  r[2] = make_double2(fn1, __longlong_as_double((long long)fl));
+}
+
 // The per-step record of an owned cell in the step's slot (fx_dev::rec32).
 __device__ __forceinline__ void put_rec32(const fx_dev& d, long long o, float h0, float h, float hp, float mm,
                                           float fe1, float fn1, uint8_t fl) {
@@ -1239,11 +1249,11 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       const uint8_t fl = d.flags[sprev + gi];
       const double hpre = fmax(0.0, zpre - zb);
       uint8_t ld = hpre > d.hdry ? 0 : 1;  // Courant scan (:308-320)
-      double z1 = zpre, h1 = hpre;
+      double z1 = zpre, h1 = hpre, hpv = 0.0;
       if (melt_on && zb != d.nodata) {
         const double mi = melt_depth(d, c, gi);
         bmelt = mi * d.arbase;
-        if (d.ade) d.hpm[scur + gi] = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
+        hpv = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
         z1 = zpre + mi;
         h1 = fmax(z1 - zb, 0.0);
         if (h1 <= d.hdry) ld = 0;  // common.cpp:219-222
@@ -1260,13 +1270,10 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       d.z[pcur + gi] = z1;
       d.qx[pcur + gi] = qx;
       d.qy[pcur + gi] = qy;
-      d.h[scur + gi] = h1;
-      d.h0[scur + gi] = h1;
-      d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
-      if (scur != sprev) {  // fluxes are unchanged by a step without solver
-        d.fe1[scur + gi] = d.fe1[sprev + gi];
-        d.fn1[scur + gi] = d.fn1[sprev + gi];
-      }
+      const uint8_t fl1 = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+      d.flags[scur + gi] = fl1;
+      const double* rp = fx_rec64(d, sprev + gi);  // fluxes are unchanged by a step without solver
+      put_rec64(d, scur + gi, h1, h1, hpv, rp[FX_R64_FE1], rp[FX_R64_FN1], fl1);
       courant_cell(d, h1, qx, qy, dtc, hm);
     }
     acc.add(dtc, hm, bmelt, 0.0);
@@ -1399,10 +1406,11 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       const int k = S.stale_list[i];
       const int fr = k % FXN, fc = k / FXN;
       const long long gi = fx_ix(d, irow0 - 1 + fr, icol0 - 1 + fc);
-      S.f[0][k] = d.fe1[sprev + gi];
+      const double* rp = fx_rec64(d, sprev + gi);
+      S.f[0][k] = rp[FX_R64_FE1];
       S.f[1][k] = d.fe2[gi];
       S.f[2][k] = d.fe3[gi];
-      S.f[3][k] = d.fn1[sprev + gi];
+      S.f[3][k] = rp[FX_R64_FN1];
       S.f[4][k] = d.fn2[gi];
       S.f[5][k] = d.fn3[gi];
     }
@@ -1427,10 +1435,10 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     // Courant scan's copy of h (main.cpp:305) for cells it skips. Its solute
     // dilution (:226-234) is applied by the ADE sweep (fx_ade.cu).
     double h0v = fmax(0.0, zpre - zb);
-    double mi = 0.0;
+    double mi = 0.0, hpv = 0.0;
     if (melt_on && zb != d.nodata) {
       h0v = fmax(z1 - zb, 0.0);
-      if (d.ade) d.hpm[scur + gi] = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
+      hpv = fmax(zpre - zb, 0.0);  // the dilution's hp (common.cpp:216)
       mi = (stg && d.melt_mult) ? (double)c.meteo_rate * reinterpret_cast<const double*>(stg + L::O_MM)[i8] /
                                       (1000. * 3600. * 24.) * c.dtfl
                                 : melt_depth(d, c, gi);
@@ -1493,11 +1501,10 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       }
     }
     d.z[pcur + gi] = z;
-    d.h[scur + gi] = h;
     d.qx[pcur + gi] = qx;
     d.qy[pcur + gi] = qy;
-    d.h0[scur + gi] = h0v;
-    d.flags[scur + gi] = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+    const uint8_t fl1 = (fl & (FX_F_WALL | FX_F_NODATA)) | ((fl & FX_F_LDRY) ? FX_F_LDRY_PREV : 0) | ld;
+    d.flags[scur + gi] = fl1;
     // Fluxes computed this step become the grid values (stale ones are
     // already there). fe_2/fe_3/fn_2/fn_3 are read back only when this cell
     // is dry with four dry neighbours at a later solver step; a cell that
@@ -1505,24 +1512,23 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     // long as forcing adds water, so those three-quarters of the flux
     // traffic are skipped for it.
     const unsigned char clP = cl;
+    double fe1v = 0.0, fn1v = 0.0;
     if ((clP & C_INT) && !(clP & C_WALL)) {
       const bool computed =
           !(clP & C_DRY) || !((S.cls[sidx(lx + 1, ly + 2)] & C_DRY) && (S.cls[sidx(lx + 3, ly + 2)] & C_DRY) &&
                               (S.cls[sidx(lx + 2, ly + 1)] & C_DRY) && (S.cls[sidx(lx + 2, ly + 3)] & C_DRY));
       // fe_1/fn_1 of every cell go to this step's slot: computed ones, or the
       // stale ones carried over (already in S.f for stale cells).
-      d.fe1[scur + gi] = S.f[0][fP];
-      d.fn1[scur + gi] = S.f[3][fP];
+      fe1v = S.f[0][fP];
+      fn1v = S.f[3][fP];
       if (computed && (d.store_all_fluxes || !(h > d.hdry))) {
         d.fe2[gi] = S.f[1][fP];
         d.fe3[gi] = S.f[2][fP];
         d.fn2[gi] = S.f[4][fP];
         d.fn3[gi] = S.f[5][fP];
       }
-    } else if (scur != sprev) {
-      d.fe1[scur + gi] = 0.0;  // walls: never written in the reference
-      d.fn1[scur + gi] = 0.0;
-    }
+    }  // walls: fe_1 = fn_1 = 0, never written in the reference
+    put_rec64(d, scur + gi, h0v, h, hpv, fe1v, fn1v, fl1);
     courant_cell(d, h, qx, qy, dtc, hm);
   }
   acc.add(dtc, hm, bmelt, bout);
@@ -1891,7 +1897,7 @@ __global__ void __launch_bounds__(BX * BY) k_courant_scan(const fx_dev* __restri
       courant_cell32(d, fmax(0.0, fx_dd_val(d.eta[pl + gi], d.eta_lo[pl + gi])), d.qx_f[pl + gi],
                      d.qy_f[pl + gi], dtc, hm);
     else
-      courant_cell(d, d.h[sl + gi], d.qx[pl + gi], d.qy[pl + gi], dtc, hm);
+      courant_cell(d, fx_rec64(d, sl + gi)[FX_R64_H], d.qx[pl + gi], d.qy[pl + gi], dtc, hm);
   }
   reduce_courant(d, S, dtc, hm);
 }
@@ -2032,7 +2038,7 @@ __global__ void __launch_bounds__(256) k_mass(const __grid_constant__ fx_dev d, 
     const int icol = (int)(i / d.ld), irow = (int)(i % d.ld) - FX_ROFF;
     if (irow < 1 || irow > d.nr || icol < 1 || icol > d.nc) continue;
     if (d.flags[sl + i] & FX_F_WALL) continue;
-    const double h = d.prec32 ? (double)fx_rec(d, sl + i)[FX_R_H] : d.h[sl + i];
+    const double h = d.prec32 ? (double)fx_rec(d, sl + i)[FX_R_H] : fx_rec64(d, sl + i)[FX_R64_H];
     acc[0] += d.prec32 ? fx_dd_val(d.eta[pl + i], d.eta_lo[pl + i]) : d.z[pl + i] - d.zb[i];
     for (int k = 0; k < d.nchem; ++k)
       acc[1 + k] += h * (d.prec32 ? (double)d.conc_f[k * d.plane + i] : d.conc[k * d.plane + i]);

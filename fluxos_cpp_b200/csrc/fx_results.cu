@@ -19,7 +19,7 @@ namespace fxres {
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ double cell_h(const fx_dev& d, long long sl, long long gi) {
-  return d.prec32 ? (double)fx_rec(d, sl + gi)[FX_R_H] : d.h[sl + gi];
+  return d.prec32 ? (double)fx_rec(d, sl + gi)[FX_R_H] : fx_rec64(d, sl + gi)[FX_R64_H];
 }
 
 __device__ __forceinline__ bool selected(const fx_dev& d, long long sl, long long gi, double hmin) {
@@ -122,8 +122,8 @@ __global__ void k_write(const __grid_constant__ fx_dev d, double hmin, const lon
           qy = d.qy[pp + gi];
           conc = d.conc[gi];
           soil = d.soil ? d.soil[gi] : 0.0;
-          fe1 = d.fe1[sl + gi];
-          fn1 = d.fn1[sl + gi];
+          fe1 = fx_rec64(d, sl + gi)[FX_R64_FE1];
+          fn1 = fx_rec64(d, sl + gi)[FX_R64_FN1];
           twet = d.twet[gi];
         }
         o.irow[k] = irow;
