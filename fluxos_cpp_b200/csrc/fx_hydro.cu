@@ -835,20 +835,16 @@ __device__ void solver_wet32(const fx_dev& d, const SM& S, int sr, int sc, int i
     if (irow == 1 || irow == d.nr) fe1 = fminf(volrat, weir);
   }
   volrat = fdiv((float)d.arbase * hp, dtl);
-  if (volrat > 0.0f) {
-    if (fe1 > 0.0f && fn1 > 0.0f) {
-      if (fe1 * dy + fn1 * dx > volrat) {
-        const float cf = fdiv(fn1 * dx, fe1 * dy + fn1 * dx);
-        fe1 = div_dxy_f(d, (1.f - cf) * volrat);
-        fn1 = div_dxy_f(d, cf * volrat);
-      }
-    } else if (fe1 > 0.0f) {
-      fe1 = div_dxy_f(d, fminf(fe1 * dy, volrat));
-    } else if (fn1 > 0.0f) {
-      fn1 = div_dxy_f(d, fminf(fn1 * dx, volrat));
-    }
-  } else {
-    fe1 = fn1 = 0.0f;
+  {  // solver_wetdomain.cpp:309-332 as selects: one straight-line block, the
+     // quotient of the split kept only when the split applies
+    const float sdy = fe1 * dy, sdx = fn1 * dx, sum = sdy + sdx;
+    const bool pos = volrat > 0.0f, pe = fe1 > 0.0f, pn = fn1 > 0.0f;
+    const bool split = pos && pe && pn && sum > volrat;
+    const float cf = fdiv(sdx, split ? sum : 1.0f);
+    const float e = div_dxy_f(d, split ? (1.f - cf) * volrat : fminf(sdy, volrat));
+    const float n = div_dxy_f(d, split ? cf * volrat : fminf(sdx, volrat));
+    fe1 = !pos ? 0.0f : ((split || (pe && !pn)) ? e : fe1);
+    fn1 = !pos ? 0.0f : ((split || (pn && !pe)) ? n : fn1);
   }
   out[0] = fe1;
   out[1] = fe2;
