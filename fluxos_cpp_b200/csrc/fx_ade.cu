@@ -83,7 +83,7 @@ template <>
 struct Ring<float> {
   static constexpr int CV = 4;
   float c[RING][32][CV];
-  float4 a[RING][32];  // h0, h, hp, melt multiplier
+  float4 a[RING][32];  // h0, h, hp, the step's melt depth
   float4 b[RING][32];  // fe_1, fn_1, flag byte (as the float's bits), 0
 };
 
@@ -297,8 +297,7 @@ __device__ __forceinline__ Rec<T> make_rec(const fx_dev& d, const StepIn& S, con
   const T hm = inflow_cell ? (T)S.inflow_hm : h0;
   if (S.dilute) {
     const T hp = ra.z;
-    // the melt depth the hydrodynamic step added (melt32 in fx_hydro.cu)
-    const T mi = Fields<T>::mm(d) ? (T)(S.meteoi * (double)ra.w) : (T)S.meteoi;
+    const T mi = ra.w;  // the melt depth the hydrodynamic step added (melt32 in fx_hydro.cu)
     const bool use = !(fl & FX_F_NODATA) && hp != T(0);  // then hm >= hp > 0
     const T cd = tdiv(c * hp + (mi * (T)S.mconc), use ? hm : T(1));
     c = use ? cd : c;

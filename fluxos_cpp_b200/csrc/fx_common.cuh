@@ -156,8 +156,8 @@ struct fx_dev {
   float *fe2_f, *fe3_f, *fn2_f, *fn3_f;
   float* conc_f;                              // nchem planes
   // FP32 state: the per-step fields (h, h0, the pre-melt depth hp, fe_1,
-  // fn_1) as one 32-byte record per cell and slot plane, {h0, h, hp, melt
-  // multiplier} then {fe_1, fn_1, flag byte (as the float's bits), 0}: the
+  // fn_1) as one 32-byte record per cell and slot plane, {h0, h, hp, the
+  // step's melt depth} then {fe_1, fn_1, flag byte (as the float's bits), 0}: the
   // ADE sweep fetches a cell's step inputs as one sector instead of one
   // sector per field (fx_ade.cu). The hydrodynamic step writes the record of
   // each interior cell; the ghost ring holds what was uploaded. Cell gi of
@@ -232,7 +232,7 @@ __host__ __device__ inline void fx_dd_add(float& hi, float& lo, float x) {
 __host__ __device__ inline double fx_dd_val(float hi, float lo) { return (double)hi + (double)lo; }
 
 // Components of the FP32 state's per-step record (fx_dev::rec32).
-enum { FX_R_H0 = 0, FX_R_H = 1, FX_R_HP = 2, FX_R_MM = 3, FX_R_FE1 = 4, FX_R_FN1 = 5, FX_R_FL = 6 };
+enum { FX_R_H0 = 0, FX_R_H = 1, FX_R_HP = 2, FX_R_MI = 3, FX_R_FE1 = 4, FX_R_FN1 = 5, FX_R_FL = 6 };
 // The record of the cell at slot-plane element o (slot offset + fx_ix).
 __host__ __device__ inline float* fx_rec(const fx_dev& d, long long o) {
   return reinterpret_cast<float*>(d.rec32 + 2 * o);

@@ -930,10 +930,10 @@ __device__ __forceinline__ void put_rec64(const fx_dev& d, long long o, double h
 }
 
 // The per-step record of an owned cell in the step's slot (fx_dev::rec32).
-__device__ __forceinline__ void put_rec32(const fx_dev& d, long long o, float h0, float h, float hp, float mm,
+__device__ __forceinline__ void put_rec32(const fx_dev& d, long long o, float h0, float h, float hp, float mi,
                                           float fe1, float fn1, uint8_t fl) {
   float4* r = d.rec32 + 2 * o;
-  r[0] = make_float4(h0, h, hp, mm);
+  r[0] = make_float4(h0, h, hp, mi);
   r[1] = make_float4(fe1, fn1, __uint_as_float((unsigned)fl), 0.0f);
 }
 
@@ -965,8 +965,10 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       uint8_t ld = fx_dd_val(etapre, lo1) > d.hdry ? 0 : 1;
       float h1 = hpre;
       double depth = fx_dd_val(etapre, lo1);
+      float mir = 0.0f;  // the record's melt depth
       if (melt_on && !(fl & FX_F_NODATA)) {
         const float mi = melt32(d, c, d.melt_mult_f ? d.melt_mult_f[gi] : 1.0f);
+        mir = mi;
         bmelt = (double)mi * d.arbase;
         fx_dd_add(eta1, lo1, mi);
         h1 = fmaxf(eta1, 0.0f);
@@ -992,7 +994,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       // fluxes are unchanged by a step without solver
       const float* rp = fx_rec(d, sprev + gi);
       const bool melted = melt_on && !(fl & FX_F_NODATA);
-      put_rec32(d, scur + gi, h1, h1, melted ? hpre : 0.0f, melted && d.melt_mult_f ? d.melt_mult_f[gi] : 1.0f,
+      put_rec32(d, scur + gi, h1, h1, melted ? hpre : 0.0f, mir,
                 rp[FX_R_FE1], rp[FX_R_FN1], fl1);
       courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
     }
@@ -1126,14 +1128,14 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     const float etapre = stg ? reinterpret_cast<const float*>(stg + L::O_Z)[i4] : d.eta[pprev + gi];
     float h0v = fmaxf(0.0f, etapre);
     double mi = 0.0;
-    float hpv = 0.0f, mmv = 1.0f;  // the ADE record's pre-melt depth and melt multiplier
+    float hpv = 0.0f, miv = 0.0f;  // the record's pre-melt depth and melt depth
     if (melt_on && !(fl & FX_F_NODATA)) {
       h0v = fmaxf(eta1, 0.0f);
       hpv = fmaxf(etapre, 0.0f);
       const float mm = !d.melt_mult_f ? 1.0f
                        : (stg ? reinterpret_cast<const float*>(stg + L::O_MM)[i4] : d.melt_mult_f[gi]);
-      mmv = mm;
-      mi = (double)melt32(d, c, mm);
+      miv = melt32(d, c, mm);
+      mi = (double)miv;
       bmelt = mi * d.arbase;
     }
     if (is_inflow(d, irow, icol)) {  // common.cpp:300-315 (h0 = the depth after the inflow)
@@ -1205,7 +1207,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         d.fn3_f[gi] = S.f[5][fP];
       }
     }
-    put_rec32(d, scur + gi, h0v, h, hpv, mmv, fe1v, fn1v, fl1);
+    put_rec32(d, scur + gi, h0v, h, hpv, miv, fe1v, fn1v, fl1);
     courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
   }
   acc.add(dtc, hm, bmelt, bout);
