@@ -84,8 +84,8 @@ ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
 # 16-row tiles, the FP64 one with 8-row tiles, the shapes the autotuner
 # picks); traffic scales with the cells, so `traffic` in the line is this
 # times the cells of the run.
-DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 151.98, "k_ade_sweep": 56.12},
-                       "fp32": {"k_hydro": 91.17, "k_ade_sweep": 34.57}}
+DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 152.81, "k_ade_sweep": 55.78},
+                       "fp32": {"k_hydro": 91.08, "k_ade_sweep": 34.86}}
 
 
 def _rank():
