@@ -34,3 +34,22 @@ def test_errors_without_a_context_are_reported():
     assert not h.value
     assert L.fx_load_modset(b"/nonexistent/modset.json", ctypes.byref(g), ctypes.byref(p), None, None,
                             None, None, None, None, None, None, None, None, None, None) == -3  # FX_ERR_IO
+
+
+def test_footprint_counts_one_record_per_cell_and_step_in_flight():
+    """fx_footprint is host arithmetic (no GPU): each step in flight adds one
+    slot of per-step state per cell, a 32-byte record and a flag byte in FP32,
+    a 48-byte record and a flag byte in FP64, plus the ADE's per-strip
+    hand-over and counters and its unit table."""
+    n = 1000
+    ld = ((n + 2 + 1 + 31) // 32) * 32
+    plane = ld * (n + 2)
+    strips = (n + 29) // 30
+    ade = 8 * strips * (n + 2) * 3 + 8 * strips + 16 * strips  # hand-over, counters, units (one solute)
+    for precision, per_cell in (("fp32", 33), ("fp64", 49)):
+        a = fx.footprint(n, n, nchem=1, precision=precision, steps_in_flight=8)
+        b = fx.footprint(n, n, nchem=1, precision=precision, steps_in_flight=9)
+        assert b - a == plane * per_cell + ade, (precision, b - a)
+    # FP32 state holds less than FP64 at the same steps in flight
+    assert fx.footprint(n, n, precision="fp32", steps_in_flight=31) < fx.footprint(n, n, precision="fp64",
+                                                                                 steps_in_flight=31)
