@@ -938,8 +938,9 @@ __device__ __forceinline__ void put_rec32(const fx_dev& d, long long o, float h0
 }
 
 template <int BY>
-__device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
-                                             HydroSmem32<BY>& S, TilePart& acc, const unsigned char* stg = nullptr) {
+__device__ __forceinline__ bool hydro_tile32(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
+                                             HydroSmem32<BY>& S, TilePart& acc, const unsigned char* stg = nullptr,
+                                             int bad = 0) {
   using L = StageLayout<true, BY>;
   const StageOff so = stage_off(tile.bx);
   constexpr int TY = Tile<BY>::TY, NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX;
@@ -999,7 +1000,7 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
       courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
     }
     acc.add(dtc, hm, bmelt, 0.0);
-    return;
+    return true;
   }
 
   if (stg) {
@@ -1081,7 +1082,9 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
         S.v[k] = fdiv(qy, den);
       }
   }
-  __syncthreads();
+  // the stencil is complete; a thread whose stage wait gave up (bad) stops
+  // the whole block here, before anything is written to global memory
+  if (__syncthreads_or(bad)) return false;
   {
     // Each thread computes its own face-flux cell (NFLUX == NTHREADS), wet,
     // dry or kept, without the FP64 path's work lists: in FP32 the lists'
@@ -1211,12 +1214,14 @@ __device__ __forceinline__ void hydro_tile32(const fx_dev& d, const StepCtl& c, 
     courant_cell32(d, fmax(0.0, depth), qx, qy, dtc, hm);
   }
   acc.add(dtc, hm, bmelt, bout);
+  return true;
 }
 
 // The FP64 step of one tile (the reference's arithmetic, bit for bit).
 template <int BY>
-__device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
-                                             HydroSmem<BY>& S, TilePart& acc, const unsigned char* stg = nullptr) {
+__device__ __forceinline__ bool hydro_tile64(const fx_dev& d, const StepCtl& c, const fx_tile& tile,
+                                             HydroSmem<BY>& S, TilePart& acc, const unsigned char* stg = nullptr,
+                                             int bad = 0) {
   using L = StageLayout<false, BY>;
   const StageOff so = stage_off(tile.bx);
   constexpr int TY = Tile<BY>::TY, NSTEN = Tile<BY>::NSTEN, NFLUX = Tile<BY>::NFLUX;
@@ -1275,7 +1280,7 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       courant_cell(d, h1, qx, qy, dtc, hm);
     }
     acc.add(dtc, hm, bmelt, 0.0);
-    return;
+    return true;
   }
 
   // ---- phase A: stencil load, melt, Loop 1 ---------------------------------
@@ -1359,7 +1364,9 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
       S.v[k] = qy / den;
     }
   }
-  __syncthreads();
+  // the stencil is complete; a thread whose stage wait gave up (bad) stops
+  // the whole block here, before anything is written to global memory
+  if (__syncthreads_or(bad)) return false;
 
   // ---- phase B: classify flux cells into warp-uniform work lists ----------
   for (int k = tid; k < NFLUX; k += NTHREADS) {
@@ -1530,6 +1537,7 @@ __device__ __forceinline__ void hydro_tile64(const fx_dev& d, const StepCtl& c, 
     courant_cell(d, h, qx, qy, dtc, hm);
   }
   acc.add(dtc, hm, bmelt, bout);
+  return true;
 }
 
 // Reads the step's fields of the control block (written by k_finalize) into
@@ -1671,7 +1679,6 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
   __shared__ HydroSmem<BY> S;
   __shared__ StepCtl sc;
   __shared__ __align__(8) unsigned long long bar[2];
-  __shared__ int abort_flag;
   extern __shared__ __align__(128) unsigned char dyn[];
   unsigned char* stage0 = dyn + ((128 - (smem_u32(dyn) & 127)) & 127);
   const int tid = threadIdx.y * BX + threadIdx.x;
@@ -1687,7 +1694,6 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
     sc.steps = g.steps;
     sc.live = g.live;
     sc.active = g.active;
-    abort_flag = 0;
   }
   __syncthreads();
   const StepCtl c = sc;
@@ -1716,17 +1722,24 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
     const int tn = t + gridDim.x;
     if (tid == 0 && tn < ntiles)
       stage_issue<P32, BY>(d, tm, tn, ntx, c.steps - 1, stage0 + (st ^ 1) * L::BYTES, &bar[st ^ 1]);
-    // wait for this tile's stencil, bounded
+    // wait for this tile's stencil, bounded; each thread waits for itself,
+    // and the tile's first barrier (after the stencil is read) tells the
+    // whole block whether any wait gave up
     long long it = 0;
+    int bad = 0;
     while (!mbar_try_wait(&bar[st], (parity >> st) & 1u)) {
       if (++it > STAGE_SPIN_LIMIT) {
-        abort_flag = 1;
+        bad = 1;
         break;
       }
     }
     parity ^= 1u << st;
-    __syncthreads();
-    if (abort_flag) {
+    const fx_tile tile{0, t % ntx, t / ntx, 0};
+    bool done;
+    if constexpr (P32)
+      done = hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S), acc, stage0 + st * L::BYTES, bad);
+    else done = hydro_tile64<BY>(d, c, tile, S, acc, stage0 + st * L::BYTES, bad);
+    if (!done) {  // every thread of the block takes this branch
       if (tid == 0) {
         atomicCAS(&d.ctl->error, 0, FX_DEVERR_WAIT_TIMEOUT);
         // let the copy of the next tile, if one was issued, land before the block exits
@@ -1737,10 +1750,6 @@ __global__ void __launch_bounds__(BX * BY, min_blocks<P32, BY>())
       }
       return;
     }
-    const fx_tile tile{0, t % ntx, t / ntx, 0};
-    if constexpr (P32)
-      hydro_tile32<BY>(d, c, tile, *reinterpret_cast<HydroSmem32<BY>*>(&S), acc, stage0 + st * L::BYTES);
-    else hydro_tile64<BY>(d, c, tile, S, acc, stage0 + st * L::BYTES);
     __syncthreads();  // the stage is free for the load issued two tiles later
     st ^= 1;
   }
