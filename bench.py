@@ -78,12 +78,11 @@ ALG_BYTES = {"fp64": {"k_hydro": 73, "k_ade_sweep": 16, "step": 89},
              "fp64_parity": {"k_hydro": 57, "k_ade_sweep": 16, "step": 73}}
 # DRAM bytes per cell that each kernel actually moves per step
 # (dram__bytes_read.sum + dram__bytes_write.sum from ncu on the 2048 x 2048
-# case of this workload, one launch, divided by the cells and the steps the
-# launch covers: profiles/k_ade_one_fractal2048.md,
-# profiles/k_hydro_tma_fractal2048.md; the FP32 hydrodynamic kernel with
+# case of this workload at 20 steps in flight, one launch, divided by the
+# cells and the steps the launch covers; the FP32 hydrodynamic kernel with
 # 16-row tiles, the FP64 one with 8-row tiles, the shapes the autotuner
-# picks); traffic scales with the cells, so `traffic` in the line is this
-# times the cells of the run.
+# picks; the captures are summarised in profiles/); traffic scales with the
+# cells, so `traffic` in the line is this times the cells of the run.
 DRAM_BYTES_PER_CELL = {"fp64": {"k_hydro": 152.81, "k_ade_sweep": 55.78},
                        "fp32": {"k_hydro": 91.08, "k_ade_sweep": 34.86}}
 
